@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""Headline benchmark: DGEMM TFLOPS on one B200, INT8-emulated (Ozaki, tcgen05
+kind::i8) vs plain FP64 (DMMA), at M=N=K=8192 on exponent-spread inputs
+a = u*exp(phi*g) (u ~ U[-1,1), g ~ N(0,1), seed 2), errors stated against the
+double-double product.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                    [--method ozaki|fp64] [--n 8192] [--phi 1.0] [--slices 0]
+
+Prints ONE JSON line (rank 0).  ``value`` is device-timed whole-job TFLOPS with
+inputs resident in HBM; ``e2e`` is the same metric through the drop-in
+``dgemm_`` C symbol with pinned host buffers (H2D + D2H inside the timed
+region).  Each 8192^2 FP64 operand is 512 MiB, larger than the 126 MB L2, so
+no flush is needed between steps.  With N > 1 each rank runs an independent
+replica (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DGEMM TFLOPS: INT8-emulated vs plain FP64 at equal oracle error, one B200"
+SM_COUNT_B200 = 148
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--method", default="ozaki", choices=["ozaki", "fp64"])
+    p.add_argument("--n", type=int, default=8192)
+    p.add_argument("--phi", type=float, default=1.0)
+    p.add_argument("--slices", type=int, default=0)
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-error", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    return p.parse_args()
+
+
+def make_inputs(n: int, phi: float, seed: int = 2):
+    """Config-3 inputs: u then g for A, then u then g for B, column-major order."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(2):
+        u = rng.uniform(-1.0, 1.0, n * n)
+        g = rng.standard_normal(n * n)
+        out.append(u * np.exp(phi * g))
+    return out[0], out[1]
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return json.load(fh), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, \
+            "fallback"
+
+
+def physical_cores() -> int:
+    try:
+        import psutil
+
+        return psutil.cpu_count(logical=False) or os.cpu_count() or 1
+    except Exception:
+        return os.cpu_count() or 1
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (read-only queries)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sms:
+            return None
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+# ------------------------------------------------------------ CPU legs ----
+def cpu_dgemm_rate(a: np.ndarray, b: np.ndarray, n: int, seconds: float):
+    """Time the reference's dgemm_ (oracle/_ref/DGEMM.so) on this host when it
+    runs here (AVX-512F), else the oracle's C port, on a column sample of the
+    same product: M = K = n, N = ncols chosen for ~`seconds` of work."""
+    from oracle import oracle as O
+
+    kind = "reference" if (O.ref_available("DGEMM.so") and O.host_has_avx512f()) else "port"
+    A = a.reshape(n, n, order="F")
+    B = b.reshape(n, n, order="F")
+
+    def run(cols):
+        c = np.zeros((n, cols), order="F")
+        bs = B[:, :cols]
+        t0 = time.perf_counter()
+        if kind == "reference":
+            O.ref_gemm("N", "N", n, cols, n, 1.0, A, bs, 0.0, c)
+        else:
+            O.gemm("N", "N", n, cols, n, 1.0, A, bs, 0.0, c)
+        return time.perf_counter() - t0
+
+    probe = 16 if kind == "port" else 64
+    run(probe)  # thread pool spin-up and first-touch pages
+    dt = run(probe)
+    rate = 2.0 * n * n * probe / dt
+    cols = int(max(probe, min(n, seconds * rate / (2.0 * n * n))))
+    dt = run(cols)
+    return {"value": 2.0 * n * n * cols / dt / 1e12, "unit": "TFLOPS",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)),
+            "kind": kind,
+            "sample": f"dgemm_ NN M=K={n}, N={cols} columns of the same B, alpha=1 beta=0, "
+                      f"{dt:.1f} s"}
+
+
+def reference_arm(args, rank: int):
+    if rank != 0:
+        return None
+    os.environ.setdefault("OMP_NUM_THREADS", str(physical_cores()))
+    a, b = make_inputs(args.n, args.phi)
+    steps = []
+    res = None
+    for i in range(args.warmup + args.steps):
+        res = cpu_dgemm_rate(a, b, args.n, seconds=max(2.0, args.cpu_seconds / 2))
+        if i >= args.warmup:
+            steps.append(res["value"])
+    val = statistics.median(steps)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_block(args),
+        "cpu_baseline": {"value": val, "unit": "TFLOPS", "cores": res["cores"],
+                         "kind": res["kind"], "sample": res["sample"]},
+        "e2e": {"value": val, "unit": "TFLOPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def config_block(args):
+    return {"workload": f"DGEMM NN M=N=K={args.n}, a=u*exp(phi*g) phi={args.phi}, "
+                        f"alpha=1 beta=0, seed 2",
+            "M": args.n, "N": args.n, "K": args.n, "phi": args.phi, "method": args.method,
+            "parallelism": f"replicas x{args.gpus}",
+            "l2": "inputs larger than L2 (512 MiB per operand), no flush"}
+
+
+# ------------------------------------------------------------- GPU arm ----
+def gpu_arm(args, rank: int, world: int):
+    import torch
+
+    from gemm_avx512f_b200 import _lib, blas
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    L = _lib.lib()
+    n = args.n
+    a_h, b_h = make_inputs(n, args.phi)
+    A = torch.from_numpy(a_h).to(dev)
+    B = torch.from_numpy(b_h).to(dev)
+    Cd = torch.zeros(n * n, dtype=torch.float64, device=dev)
+    # An explicit stream: handle 0 (torch's legacy default stream) would mean
+    # "the library's own stream" to libb2blas and escape the events below.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sptr = stream.cuda_stream
+    method = _lib.METHODS[args.method]
+    flops = 2.0 * n * n * n
+
+    def step(meth=method, slices=args.slices):
+        st = L.b2_dgemm(b"N", b"N", n, n, n, 1.0, A.data_ptr(), n, B.data_ptr(), n, 0.0,
+                        Cd.data_ptr(), n, meth, slices, sptr)
+        if st != 0:
+            raise _lib.B2Error(st, L.b2_last_info(), "b2_dgemm")
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(dev.index)
+    clocks.start()
+    _lib.profile_enable(True)
+    _lib.profile_report()  # drop warm-up records
+    n0 = _lib.launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = _lib.launch_count() - n0
+    prof = _lib.profile_report()
+    _lib.profile_enable(False)
+    ck = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * flops * args.steps / (ms / 1e3) / 1e12
+
+    # ---- dominant kernel roofline (live CUDA-event durations over the timed region)
+    peaks, peak_src = load_peaks()
+    roof = None
+    if prof:
+        top = max(prof.items(), key=lambda kv: kv[1][1])
+        kname, (kcnt, kms) = top
+        avg_s = kms / kcnt / 1e3
+        if kname.startswith("ozaki_i8_gemm"):
+            ops = flops * ozaki_info(L)["moduli"]
+            peak = 2.0 * peaks["bf16_tflops"]
+            roof = {"bound": "tensor", "kernel": kname, "unit": "TFLOP/s",
+                    "achieved": ops / avg_s / 1e12, "peak": peak,
+                    "peak_source": f"INT8 dense = 2 x {peak_src} bf16 ({peaks['bf16_tflops']})"}
+        elif kname.startswith("dgemm_dmma"):
+            peak = SM_COUNT_B200 * 128 * 1.965e9 / 1e12
+            roof = {"bound": "tensor", "kernel": kname, "unit": "TFLOP/s",
+                    "achieved": flops / avg_s / 1e12, "peak": peak,
+                    "peak_source": "nominal FP64 dense (148 SM x 128 FLOP/clk x 1.965 GHz); "
+                                   "no measured FP64 peak"}
+        if roof:
+            roof["frac"] = roof["achieved"] / roof["peak"]
+            roof["traffic"] = profile_traffic(kname)
+            roof["kernel_share"] = kms / ms if ms else None
+            roof["launches_timed"] = kcnt
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "TFLOPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config_block(args), "roofline": roof,
+        "gpu_launches": launches, "clocks": ck,
+        "kernels": {k: {"launches": v[0], "ms": v[1]} for k, v in prof.items()},
+    }
+    if args.method == "ozaki":
+        out["ozaki"] = ozaki_info(L)
+
+    # ---- plain FP64 on the same inputs (the comparison the metric names)
+    if args.method == "ozaki":
+        for _ in range(2):
+            step(_lib.METHODS["fp64"], 0)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        k2 = max(2, min(args.steps, 5))
+        for _ in range(k2):
+            step(_lib.METHODS["fp64"], 0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out["fp64_tflops"] = flops * k2 / (e0.elapsed_time(e1) / 1e3) / 1e12
+        out["speedup_vs_fp64"] = value / world / out["fp64_tflops"]
+
+    # ---- errors vs the double-double product (computed once, outside timing)
+    if not args.no_error and rank == 0:
+        errs = {}
+        hi = torch.empty(n * n, dtype=torch.float64, device=dev)
+        blas.dgemm_dd_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, None, n, hi, None, n,
+                             stream=stream)
+        meths = ["fp64", "ozaki"] if args.method == "ozaki" else ["fp64"]
+        for mth in meths:
+            step(_lib.METHODS[mth], args.slices if mth == "ozaki" else 0)
+            torch.cuda.synchronize()
+            d = Cd - hi
+            errs[mth] = {"normwise": float(torch.linalg.vector_norm(d) /
+                                           torch.linalg.vector_norm(hi)),
+                         "max_elementwise": float(d.abs().max() / hi.abs().max())}
+        if "ozaki" in errs:
+            errs["ozaki_over_fp64_normwise"] = errs["ozaki"]["normwise"] / \
+                errs["fp64"]["normwise"]
+        out["errors_vs_dd"] = errs
+        del hi
+
+    # ---- end to end through the drop-in dgemm_ with pinned host buffers
+    if not args.no_e2e:
+        out["e2e"] = e2e_leg(args, L, a_h, b_h, method)
+
+    # ---- CPU baseline (reference on the host cores), rank 0 at N=1 only
+    if not args.no_cpu and rank == 0 and world == 1:
+        try:
+            out["cpu_baseline"] = cpu_dgemm_rate(a_h, b_h, n, args.cpu_seconds)
+        except Exception as exc:  # keep the GPU line even if the CPU leg cannot run
+            out["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    return out
+
+
+def ozaki_info(L) -> dict:
+    info = {}
+    try:
+        L.b2_ozaki_last_plan.argtypes = [C.c_void_p, C.c_int]
+        buf = (C.c_int * 8)()
+        L.b2_ozaki_last_plan(buf, 8)
+        info = {"moduli": int(buf[0]), "k_chunks": int(buf[1])}
+    except AttributeError:
+        info = {"moduli": 0}
+    return info
+
+
+def profile_traffic(kname: str):
+    """DRAM bytes per launch of `kname` from the committed ncu summary, if any."""
+    pdir = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith(".md"):
+            continue
+        with open(os.path.join(pdir, fn)) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch:") and kname.split("<")[0] in fn:
+                    try:
+                        return float(line.split(":", 1)[1].split()[0])
+                    except ValueError:
+                        return None
+    return None
+
+
+def e2e_leg(args, L, a_h, b_h, method):
+    import torch
+
+    n = args.n
+    pa = torch.from_numpy(a_h).pin_memory()
+    pb = torch.from_numpy(b_h).pin_memory()
+    pc = torch.zeros(n * n, dtype=torch.float64).pin_memory()
+    L.b2_set_dgemm_method(method, args.slices)
+    ip = lambda v: C.byref(C.c_int(v))
+    one, zero = C.c_double(1.0), C.c_double(0.0)
+
+    def call():
+        L.dgemm_(b"N", b"N", ip(n), ip(n), ip(n), C.byref(one), pa.data_ptr(), ip(n),
+                 pb.data_ptr(), ip(n), C.byref(zero), pc.data_ptr(), ip(n))
+        if L.b2_last_error() != 0:
+            raise RuntimeError(f"dgemm_ failed: {L.b2_last_error()}")
+
+    call()
+    steps = max(2, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    dt = (time.perf_counter() - t0) / steps
+    L.b2_set_dgemm_method(_lib_fp64(), 0)
+    return {"value": 2.0 * n ** 3 / dt / 1e12, "unit": "TFLOPS",
+            "h2d_bytes_per_step": 3 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
+            "ms_per_step": dt * 1e3,
+            "note": "drop-in dgemm_ on pinned host A, B, C (C is read: beta==0 keeps NaN)"}
+
+
+def _lib_fp64():
+    from gemm_avx512f_b200 import _lib
+
+    return _lib.METHODS["fp64"]
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
+    if args.impl == "reference":
+        line = reference_arm(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        out = gpu_arm(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,423 @@
+// api.cu -- the C ABI of libb2blas.so: per-thread context, argument checks,
+// host/device pointer handling, and the drop-in Fortran-BLAS symbols.
+//
+// The drop-in symbols keep the reference's contract (src/gemm_driver.c:116):
+// void return, everything by pointer, synchronous.  Where the reference
+// allocates packing buffers per call (src/gemm_driver.c:133-140) this layer
+// keeps grow-only device workspaces per host thread, and where the reference
+// splits N across OpenMP threads (:136-149) the kernels' CTA grid does.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "b2_internal.cuh"
+#include "b2_methods.cuh"
+
+namespace b2 {
+
+static thread_local Status g_status;
+static thread_local Ctx *g_ctx = nullptr;
+
+static void set_status(int code, int info = 0) {
+  g_status.code = code;
+  g_status.info = info;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  if (getenv("B2_VERBOSE")) fprintf(stderr, "b2blas: %s failed: %s\n", what, cudaGetErrorString(e));
+  (void)cudaGetLastError();  // clear sticky-free errors so the next call starts clean
+  return B2_ERR_CUDA;
+}
+
+namespace {
+struct CtxOwner {
+  Ctx *c = nullptr;
+  ~CtxOwner() {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < WS_COUNT; ++i)
+      if (c->ws[i]) cudaFree(c->ws[i]);
+    if (c->derr) cudaFree(c->derr);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+  }
+};
+thread_local CtxOwner g_owner;
+
+int method_from_env(const char *v, int dflt) {
+  if (!v) return dflt;
+  if (!strcmp(v, "fp64")) return B2_METHOD_FP64;
+  if (!strcmp(v, "ozaki")) return B2_METHOD_OZAKI;
+  if (!strcmp(v, "auto")) return B2_METHOD_AUTO;
+  if (!strcmp(v, "fp32")) return B2_METHOD_FP32;
+  if (!strcmp(v, "tf32")) return B2_METHOD_TF32;
+  if (!strcmp(v, "tf32x3")) return B2_METHOD_TF32X3;
+  if (!strcmp(v, "bf16x3")) return B2_METHOD_BF16X3;
+  return dflt;
+}
+}  // namespace
+
+Ctx *ctx() {
+  if (g_ctx) {
+    cudaSetDevice(g_ctx->device);
+    return g_ctx;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { (void)cudaGetLastError(); return nullptr; }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) { (void)cudaGetLastError(); return nullptr; }
+  if (prop.major < 10) return nullptr;  // sm_100a code only
+  Ctx *c = new Ctx();
+  c->device = dev;
+  c->sm_count = prop.multiProcessorCount;
+  c->cc_major = prop.major;
+  c->cc_minor = prop.minor;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&c->derr, 64) != cudaSuccess || cudaMemset(c->derr, 0, 64) != cudaSuccess ||
+      cudaMallocHost(&c->pinned, 4096) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete c;
+    return nullptr;
+  }
+  c->dgemm_method = method_from_env(getenv("B2_METHOD"), B2_METHOD_FP64);
+  c->sgemm_method = method_from_env(getenv("B2_SGEMM_METHOD"), B2_METHOD_FP32);
+  if (const char *s = getenv("B2_SLICES")) c->dgemm_slices = atoi(s);
+  g_ctx = c;
+  g_owner.c = c;
+  return c;
+}
+
+void *workspace(Ctx *c, int slot, size_t bytes) {
+  if (bytes == 0) bytes = 256;
+  if (c->ws_bytes[slot] >= bytes) return c->ws[slot];
+  if (c->ws[slot]) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->ws[slot]);
+    c->ws[slot] = nullptr;
+    c->ws_bytes[slot] = 0;
+  }
+  size_t want = bytes + bytes / 8;
+  want = (want + 4095) & ~(size_t)4095;
+  void *p = nullptr;
+  if (cudaMalloc(&p, want) != cudaSuccess) {
+    (void)cudaGetLastError();
+    if (cudaMalloc(&p, bytes) != cudaSuccess) { (void)cudaGetLastError(); return nullptr; }
+    want = bytes;
+  }
+  c->ws[slot] = p;
+  c->ws_bytes[slot] = want;
+  return p;
+}
+
+cudaStream_t pick_stream(Ctx *c, void *user_stream) {
+  return user_stream ? (cudaStream_t)user_stream : c->stream;
+}
+
+// ------------------------------------------------------ pointer staging --
+bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { (void)cudaGetLastError(); return false; }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int stage_in(Ctx *c, int slot, const void *host, int rows, int cols, int ld, size_t elem,
+             void **dev, int *dld, cudaStream_t s) {
+  const int ldd = (rows + 1) & ~1;  // even leading dimension keeps 16-B vector loads legal
+  void *d = workspace(c, slot, (size_t)(ldd > 0 ? ldd : 2) * (cols > 0 ? cols : 1) * elem);
+  if (!d) return B2_ERR_NOMEM;
+  if (rows > 0 && cols > 0)
+    B2_CUDA_TRY(cudaMemcpy2DAsync(d, (size_t)ldd * elem, host, (size_t)ld * elem, (size_t)rows * elem,
+                                  cols, cudaMemcpyHostToDevice, s));
+  *dev = d;
+  *dld = ldd > 0 ? ldd : 2;
+  return B2_OK;
+}
+
+int stage_out(void *host, int ld, const void *dev, int dld, int rows, int cols, size_t elem,
+              cudaStream_t s) {
+  if (rows > 0 && cols > 0)
+    B2_CUDA_TRY(cudaMemcpy2DAsync(host, (size_t)ld * elem, dev, (size_t)dld * elem, (size_t)rows * elem,
+                                  cols, cudaMemcpyDeviceToHost, s));
+  return B2_OK;
+}
+
+static bool notrans(char c) { return c == 'N' || c == 'n'; }
+
+// BLAS argument check for xGEMM (positions as in the Fortran interface).
+int check_gemm(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc, const void *a,
+               const void *b, const void *c, int *info) {
+  const int nrowa = notrans(ta) ? m : k;
+  const int nrowb = notrans(tb) ? k : n;
+  *info = 0;
+  if (m < 0) *info = 3;
+  else if (n < 0) *info = 4;
+  else if (k < 0) *info = 5;
+  else if (lda < (nrowa > 1 ? nrowa : 1)) *info = 8;
+  else if (ldb < (nrowb > 1 ? nrowb : 1)) *info = 10;
+  else if (ldc < (m > 1 ? m : 1)) *info = 13;
+  else if (m > 0 && n > 0 && !c) *info = 12;
+  else if (m > 0 && n > 0 && k > 0 && (!a || !b)) *info = !a ? 7 : 9;
+  return *info ? B2_ERR_ARG : B2_OK;
+}
+
+// ------------------------------------------------------- DGEMM dispatch --
+int dgemm_device(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                 const double *B, int ldb, double beta, double *C, int ldc, int method,
+                 int slices, cudaStream_t s) {
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  if (method == B2_METHOD_DEFAULT) method = c->dgemm_method;
+  if (slices <= 0) slices = c->dgemm_slices;
+  if (method == B2_METHOD_AUTO) method = select_dgemm_method(c, ta, tb, m, n, k, &slices);
+  if (method == B2_METHOD_OZAKI)
+    return dgemm_ozaki(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices, s);
+  return dgemm_fp64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s, nullptr);
+}
+
+int sgemm_device(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                 const float *B, int ldb, float beta, float *C, int ldc, int method,
+                 cudaStream_t s) {
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  if (method == B2_METHOD_DEFAULT) method = c->sgemm_method;
+  return sgemm_dispatch(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method, s);
+}
+
+// Shared host-or-device driver for the real drop-in GEMMs.
+template <typename T, typename F>
+static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *a, int lda,
+                       const T *b, int ldb, T beta, T *cm, int ldc, F &&run) {
+  int info = 0;
+  int st = check_gemm(ta, tb, m, n, k, lda, ldb, ldc, a, b, cm, &info);
+  if (st != B2_OK) { set_status(st, info); return st; }
+  if (m == 0 || n == 0) { set_status(B2_OK); return B2_OK; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  cudaStream_t s = c->stream;
+  const bool need_ab = (k > 0 && alpha != (T)0);
+  const bool dev = is_device_ptr(cm) && (!need_ab || (is_device_ptr(a) && is_device_ptr(b)));
+  if (dev) {
+    st = run(a, lda, b, ldb, cm, ldc, s);
+  } else {
+    const int ra = notrans(ta) ? m : k, ca = notrans(ta) ? k : m;
+    const int rb = notrans(tb) ? k : n, cb = notrans(tb) ? n : k;
+    void *da = nullptr, *db = nullptr, *dc = nullptr;
+    int dla = 2, dlb = 2, dlc = 2;
+    st = B2_OK;
+    if (need_ab) {
+      st = stage_in(c, WS_STAGE_A, a, ra, ca, lda, sizeof(T), &da, &dla, s);
+      if (st == B2_OK) st = stage_in(c, WS_STAGE_B, b, rb, cb, ldb, sizeof(T), &db, &dlb, s);
+    }
+    if (st == B2_OK) st = stage_in(c, WS_STAGE_C, cm, m, n, ldc, sizeof(T), &dc, &dlc, s);
+    if (st == B2_OK) st = run((const T *)da, dla, (const T *)db, dlb, (T *)dc, dlc, s);
+    if (st == B2_OK) st = stage_out(cm, ldc, dc, dlc, m, n, sizeof(T), s);
+  }
+  if (st == B2_OK) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_fail(e, "stream sync");
+  }
+  set_status(st);
+  return st;
+}
+
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" {
+
+int b2_last_error(void) { return g_status.code; }
+int b2_last_info(void) { return g_status.info; }
+int b2_version(void) { return 100; }
+
+const char *b2_status_string(int s) {
+  switch (s) {
+    case B2_OK: return "ok";
+    case B2_ERR_ARG: return "invalid argument";
+    case B2_ERR_CUDA: return "CUDA runtime error";
+    case B2_ERR_NOMEM: return "device allocation failed";
+    case B2_ERR_TIMEOUT: return "bounded device wait gave up";
+    case B2_ERR_UNSUPPORTED: return "unsupported method or shape";
+    case B2_ERR_NO_DEVICE: return "no sm_100 device";
+    default: return "unknown status";
+  }
+}
+
+int b2_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) { (void)cudaGetLastError(); return 0; }
+  int ok = 0;
+  for (int i = 0; i < n; ++i) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, i) == cudaSuccess && p.major >= 10) ++ok;
+  }
+  return ok;
+}
+
+int b2_set_dgemm_method(int method, int slices) {
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  if (!(method == B2_METHOD_FP64 || method == B2_METHOD_OZAKI || method == B2_METHOD_AUTO ||
+        method == B2_METHOD_DEFAULT) || slices < 0 || slices > B2_MAX_MODULI)
+    return B2_ERR_ARG;
+  c->dgemm_method = method == B2_METHOD_DEFAULT ? B2_METHOD_FP64 : method;
+  c->dgemm_slices = slices;
+  return B2_OK;
+}
+
+int b2_set_sgemm_method(int method) {
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  if (!(method == B2_METHOD_FP32 || method == B2_METHOD_TF32 || method == B2_METHOD_TF32X3 ||
+        method == B2_METHOD_BF16X3 || method == B2_METHOD_DEFAULT))
+    return B2_ERR_ARG;
+  c->sgemm_method = method == B2_METHOD_DEFAULT ? B2_METHOD_FP32 : method;
+  return B2_OK;
+}
+
+void dgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+            const double *alpha, const double *a, const int *lda, const double *b,
+            const int *ldb, const double *beta, double *c, const int *ldc) {
+  if (!transa || !transb || !m || !n || !k || !alpha || !lda || !ldb || !beta || !ldc) {
+    set_status(B2_ERR_ARG, 0);
+    return;
+  }
+  const char ta = *transa, tb = *transb;
+  const double al = *alpha, be = *beta;
+  gemm_dropin<double>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
+                      [&](const double *A, int la, const double *B, int lb, double *C, int lc,
+                          cudaStream_t s) {
+                        return dgemm_device(ta, tb, *m, *n, *k, al, A, la, B, lb, be, C, lc,
+                                            B2_METHOD_DEFAULT, 0, s);
+                      });
+}
+
+void sgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+            const float *alpha, const float *a, const int *lda, const float *b, const int *ldb,
+            const float *beta, float *c, const int *ldc) {
+  if (!transa || !transb || !m || !n || !k || !alpha || !lda || !ldb || !beta || !ldc) {
+    set_status(B2_ERR_ARG, 0);
+    return;
+  }
+  const char ta = *transa, tb = *transb;
+  const float al = *alpha, be = *beta;
+  gemm_dropin<float>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
+                     [&](const float *A, int la, const float *B, int lb, float *C, int lc,
+                         cudaStream_t s) {
+                       return sgemm_device(ta, tb, *m, *n, *k, al, A, la, B, lb, be, C, lc,
+                                           B2_METHOD_DEFAULT, s);
+                     });
+}
+
+void SGEMM_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+            const float *alpha, const float *a, const int *lda, const float *b, const int *ldb,
+            const float *beta, float *c, const int *ldc) {
+  sgemm_(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha, const double *A,
+             int lda, const double *B, int ldb, double beta, double *C, int ldc, int method,
+             int slices, void *stream) {
+  int info = 0;
+  int st = check_gemm(transa, transb, m, n, k, lda, ldb, ldc, A, B, C, &info);
+  if (st != B2_OK) { set_status(st, info); return st; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  if (m > 0 && n > 0 &&
+      (!is_device_ptr(C) || (k > 0 && alpha != 0.0 && (!is_device_ptr(A) || !is_device_ptr(B))))) {
+    set_status(B2_ERR_ARG, !is_device_ptr(C) ? 12 : (!is_device_ptr(A) ? 7 : 9));
+    return B2_ERR_ARG;
+  }
+  st = dgemm_device(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method, slices,
+                    pick_stream(c, stream));
+  set_status(st);
+  return st;
+}
+
+int b2_sgemm(char transa, char transb, int m, int n, int k, float alpha, const float *A,
+             int lda, const float *B, int ldb, float beta, float *C, int ldc, int method,
+             void *stream) {
+  int info = 0;
+  int st = check_gemm(transa, transb, m, n, k, lda, ldb, ldc, A, B, C, &info);
+  if (st != B2_OK) { set_status(st, info); return st; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  if (m > 0 && n > 0 &&
+      (!is_device_ptr(C) || (k > 0 && alpha != 0.0f && (!is_device_ptr(A) || !is_device_ptr(B))))) {
+    set_status(B2_ERR_ARG, !is_device_ptr(C) ? 12 : (!is_device_ptr(A) ? 7 : 9));
+    return B2_ERR_ARG;
+  }
+  st = sgemm_device(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method,
+                    pick_stream(c, stream));
+  set_status(st);
+  return st;
+}
+
+int b2_dgemm_dd(char transa, char transb, int m, int n, int k, double alpha, const double *A,
+                int lda, const double *B, int ldb, double beta, const double *C0, int ldc,
+                double *Chi, double *Clo, int ldo, void *stream) {
+  int info = 0;
+  int st = check_gemm(transa, transb, m, n, k, lda, ldb, C0 ? ldc : (m > 1 ? m : 1), A, B, Chi,
+                      &info);
+  if (st == B2_OK && ldo < (m > 1 ? m : 1)) { st = B2_ERR_ARG; info = 16; }
+  if (st != B2_OK) { set_status(st, info); return st; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  st = dgemm_dd(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C0, ldc, Chi, Clo, ldo,
+                pick_stream(c, stream));
+  set_status(st);
+  return st;
+}
+
+int b2_dgemm_error(char transa, char transb, int m, int n, int k, double alpha,
+                   const double *A, int lda, const double *B, int ldb, double beta,
+                   const double *C0, const double *C, int ldc, double *normwise,
+                   double *maxelem, void *stream) {
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  if (m <= 0 || n <= 0) {
+    if (normwise) *normwise = 0.0;
+    if (maxelem) *maxelem = 0.0;
+    set_status(B2_OK);
+    return B2_OK;
+  }
+  cudaStream_t s = pick_stream(c, stream);
+  double *ref = (double *)workspace(c, WS_ERR, (size_t)m * n * sizeof(double) + 64);
+  if (!ref) { set_status(B2_ERR_NOMEM); return B2_ERR_NOMEM; }
+  double *acc = ref + (size_t)m * n;
+  int st = dgemm_dd(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C0, ldc, ref, nullptr, m, s);
+  if (st == B2_OK) st = error_stats(m, n, C, ldc, ref, m, acc, s);
+  double h[4] = {0, 0, 0, 0};
+  if (st == B2_OK) {
+    cudaError_t e = cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_fail(e, "error stats");
+  }
+  if (st == B2_OK) {
+    if (normwise) *normwise = h[1] > 0 ? sqrt(h[0] / h[1]) : sqrt(h[0]);
+    if (maxelem) *maxelem = h[3] > 0 ? h[2] / h[3] : h[2];
+  }
+  set_status(st);
+  return st;
+}
+
+int b2_device_error(int clear) {
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  int v = 0;
+  if (cudaMemcpyAsync(c->pinned, c->derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return B2_ERR_CUDA;
+  }
+  v = *(int *)c->pinned;
+  if (clear) cudaMemsetAsync(c->derr, 0, 64, c->stream), cudaStreamSynchronize(c->stream);
+  return v;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+// b2_internal.cuh -- shared declarations of libb2blas.so (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/b2blas.h"
+
+namespace b2 {
+
+// ---------------------------------------------------------------- status --
+struct Status {
+  int code = B2_OK;
+  int info = 0;
+};
+
+#define B2_CUDA_TRY(expr)                                   \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) return ::b2::cuda_fail(_e, #expr); \
+  } while (0)
+
+int cuda_fail(cudaError_t e, const char *what);  // records, returns B2_ERR_CUDA
+
+// ------------------------------------------------------------- context --
+// One per host thread: the device, a non-blocking stream, grow-only device
+// workspaces (one per slot so nested users do not alias), and the device
+// error word written by kernels whose bounded waits gave up.
+enum WsSlot {
+  WS_STAGE_A = 0, WS_STAGE_B, WS_STAGE_C,   // host-pointer staging
+  WS_OZ_X, WS_OZ_Y, WS_OZ_R, WS_OZ_SCALE,   // Ozaki slices / residues / exponents
+  WS_SPLIT_X, WS_SPLIT_Y,                   // SGEMM split planes
+  WS_TRSM, WS_3M, WS_GROUP, WS_ERR, WS_MISC,
+  WS_COUNT
+};
+
+struct Ctx {
+  int device = -1;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  cudaStream_t stream = nullptr;
+  void *ws[WS_COUNT] = {};
+  size_t ws_bytes[WS_COUNT] = {};
+  int *derr = nullptr;        // device error word
+  void *pinned = nullptr;     // small pinned scratch for host reads
+  int dgemm_method = B2_METHOD_FP64;
+  int dgemm_slices = 0;
+  int sgemm_method = B2_METHOD_FP32;
+  int fp64_override = 0;      // non-zero: use fp64_cfg for every FP64 GEMM
+};
+
+Ctx *ctx();                          // initialises on first use; nullptr if no device
+void *workspace(Ctx *c, int slot, size_t bytes);  // nullptr on allocation failure
+cudaStream_t pick_stream(Ctx *c, void *user_stream);
+
+// ------------------------------------------------------------- kernels --
+// Every launcher takes device pointers, enqueues on `s` and returns a
+// b2_status.  Dimensions are validated by the API layer.
+
+// Plain FP64 GEMM on the DMMA tensor-core path (dgemm_fp64.cu).
+struct Fp64Cfg {
+  int tile = 0;    // 0: 128x128, 1: 128x64, 2: 64x64
+  int mmak = 4;    // DMMA K shape: 4, 8 or 16
+  int split_k = 1; // >1: K split across CTAs, reduced in FP64 workspace
+};
+int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+               const double *B, int ldb, double beta, double *C, int ldc, cudaStream_t s,
+               const Fp64Cfg *cfg);
+Fp64Cfg fp64_default_cfg(int m, int n, int k, int sm_count);
+Fp64Cfg &fp64_override_cfg();
+
+// C <- beta*C (reference semantics: only called when beta != 1).
+int scale_matrix_d(int m, int n, double beta, double *C, int ldc, cudaStream_t s);
+int scale_matrix_s(int m, int n, float beta, float *C, int ldc, cudaStream_t s);
+
+// Double-double GEMM (dd_gemm.cu).
+int dgemm_dd(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+             const double *B, int ldb, double beta, const double *C0, int ldc, double *Chi,
+             double *Clo, int ldo, cudaStream_t s);
+// Error reduction of C vs Chi: sums ||C-Chi||^2, ||Chi||^2, max|C-Chi|, max|Chi| into out[4].
+int error_stats(int m, int n, const double *C, int ldc, const double *Ref, int ldr, double *out,
+                cudaStream_t s);
+
+}  // namespace b2

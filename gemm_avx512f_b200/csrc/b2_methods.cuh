@@ -1,0 +1,42 @@
+// b2_methods.cuh -- method-level entry points shared by the API layer.
+#pragma once
+
+#include "b2_internal.cuh"
+
+#define B2_MAX_MODULI 20
+
+namespace b2 {
+
+bool is_device_ptr(const void *p);
+int stage_in(Ctx *c, int slot, const void *host, int rows, int cols, int ld, size_t elem,
+             void **dev, int *dld, cudaStream_t s);
+int stage_out(void *host, int ld, const void *dev, int dld, int rows, int cols, size_t elem,
+              cudaStream_t s);
+int check_gemm(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc, const void *a,
+               const void *b, const void *c, int *info);
+
+// DGEMM dispatch on device pointers (method may be DEFAULT/AUTO).
+int dgemm_device(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                 const double *B, int ldb, double beta, double *C, int ldc, int method,
+                 int slices, cudaStream_t s);
+int sgemm_device(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                 const float *B, int ldb, float beta, float *C, int ldc, int method,
+                 cudaStream_t s);
+
+// Method selection for B2_METHOD_AUTO (selector.cu).
+int select_dgemm_method(Ctx *c, char ta, char tb, int m, int n, int k, int *slices);
+
+// INT8 Ozaki emulation of DGEMM (ozaki.cu).  slices = modulus count, 0 = auto.
+int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+                const double *B, int ldb, double beta, double *C, int ldc, int slices,
+                cudaStream_t s);
+int ozaki_auto_moduli(int k);
+
+// SGEMM methods (sgemm.cu).
+int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                   const float *B, int ldb, float beta, float *C, int ldc, int method,
+                   cudaStream_t s);
+int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+               const float *B, int ldb, float beta, float *C, int ldc, cudaStream_t s);
+
+}  // namespace b2

@@ -1,0 +1,96 @@
+// profile.cu -- launch counting and optional per-kernel CUDA-event timing.
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "b2_internal.cuh"
+#include "b2_profile.cuh"
+
+namespace b2 {
+
+static std::atomic<long long> g_launches{0};
+
+namespace {
+struct Rec {
+  const char *name;
+  cudaEvent_t a, b;
+};
+struct ProfState {
+  bool on = false;
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> pool;
+  ~ProfState() {
+    for (auto &r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+  cudaEvent_t get() {
+    if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) { (void)cudaGetLastError(); return nullptr; }
+    return e;
+  }
+};
+thread_local ProfState g_prof;
+}  // namespace
+
+ProfScope::ProfScope(const char *name, cudaStream_t s) : name_(name), s_(s) {
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!g_prof.on) return;
+  a_ = g_prof.get();
+  if (a_) cudaEventRecord((cudaEvent_t)a_, s);
+}
+
+ProfScope::~ProfScope() {
+  if (!a_) return;
+  cudaEvent_t b = g_prof.get();
+  if (!b) return;
+  cudaEventRecord(b, s_);
+  g_prof.recs.push_back(Rec{name_, (cudaEvent_t)a_, b});
+}
+
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" {
+
+long long b2_launch_count(void) { return g_launches.load(); }
+
+int b2_profile_enable(int on) {
+  g_prof.on = on != 0;
+  return B2_OK;
+}
+
+int b2_profile_report(char *buf, int len) {
+  std::map<std::string, std::pair<long, double>> agg;
+  for (auto &r : g_prof.recs) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+      auto &v = agg[r.name];
+      v.first += 1;
+      v.second += ms;
+    } else {
+      (void)cudaGetLastError();
+    }
+    g_prof.pool.push_back(r.a);
+    g_prof.pool.push_back(r.b);
+  }
+  g_prof.recs.clear();
+  if (buf && len > 0) {
+    buf[0] = 0;
+    int off = 0;
+    for (auto &kv : agg) {
+      int w = snprintf(buf + off, (size_t)(len - off), "%s %ld %.6f\n", kv.first.c_str(),
+                       kv.second.first, kv.second.second);
+      if (w < 0 || off + w >= len) break;
+      off += w;
+    }
+  }
+  return (int)agg.size();
+}
+
+}  // extern "C"

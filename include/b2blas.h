@@ -1,0 +1,200 @@
+/*
+ * b2blas.h -- C ABI of libb2blas.so, the B200 (sm_100a) dense BLAS-3 library.
+ *
+ * Two layers:
+ *   1. Drop-in Fortran-BLAS symbols with the exact signatures of the reference
+ *      (column-major, every argument by pointer, int32 dimensions, no hidden
+ *      string-length arguments).  Host or device pointers are accepted; host
+ *      buffers are staged through device memory and the call is synchronous.
+ *      These return void like the reference; argument errors and CUDA errors
+ *      never abort -- they leave C untouched and are reported by
+ *      b2_last_error() / b2_last_info() on the calling thread.
+ *   2. Extended b2_* entry points on DEVICE pointers, ordered on a caller
+ *      stream (cudaStream_t passed as void*; NULL = the library's per-thread
+ *      stream), returning a b2_status.
+ *
+ * Conventions shared with the reference (src/gemm_driver.c:18-19,131-132):
+ *   - trans char 'N'/'n' = no transpose, any other char = transpose;
+ *   - beta != 1 multiplies C by beta, so beta == 0 keeps a NaN already in C;
+ *   - alpha == 0 skips the product (C is only scaled by beta).
+ */
+#ifndef B2BLAS_H
+#define B2BLAS_H
+
+#if defined(B2_BUILD) && defined(__GNUC__)
+#define B2_API __attribute__((visibility("default")))
+#else
+#define B2_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status                                                                    */
+/* ------------------------------------------------------------------------ */
+enum b2_status {
+  B2_OK = 0,
+  B2_ERR_ARG = 1,          /* invalid argument; b2_last_info() = its 1-based position */
+  B2_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  B2_ERR_NOMEM = 3,        /* device or pinned allocation failed */
+  B2_ERR_TIMEOUT = 4,      /* a bounded device-side wait gave up; results invalid */
+  B2_ERR_UNSUPPORTED = 5,  /* method/shape combination not available */
+  B2_ERR_NO_DEVICE = 6     /* no sm_100 device visible */
+};
+
+/* Method selectors. */
+enum b2_method {
+  B2_METHOD_DEFAULT = 0,   /* library default for the routine */
+  B2_METHOD_FP64 = 1,      /* plain FP64 (DMMA tensor-core path) */
+  B2_METHOD_OZAKI = 2,     /* INT8 Ozaki emulation of FP64 (tcgen05 kind::i8) */
+  B2_METHOD_AUTO = 3,      /* selector picks method, tile config and slice count */
+  B2_METHOD_FP32 = 10,     /* SGEMM: native FP32 on the CUDA cores */
+  B2_METHOD_TF32 = 11,     /* SGEMM: 1xTF32 on tcgen05 kind::tf32, FP32 accumulate */
+  B2_METHOD_TF32X3 = 12,   /* SGEMM: split 3xTF32, FP32 accumulate */
+  B2_METHOD_BF16X3 = 13    /* SGEMM: split 3xBF16 on tcgen05 kind::f16, FP32 accumulate */
+};
+
+B2_API int b2_last_error(void);                 /* status of the last call on this thread */
+B2_API int b2_last_info(void);                  /* xerbla-style argument position, 0 if none */
+B2_API const char *b2_status_string(int status);
+B2_API int b2_device_count(void);               /* visible sm_100 devices */
+B2_API int b2_version(void);                    /* MAJOR*10000 + MINOR*100 + PATCH */
+
+/* Default method of the drop-in dgemm_ (B2_METHOD_FP64 / _OZAKI / _AUTO) and the
+ * Ozaki slice (modulus) count, 0 = chosen per call from K and the requested
+ * accuracy.  Also settable by env B2_METHOD=fp64|ozaki|auto, B2_SLICES=n. */
+B2_API int b2_set_dgemm_method(int method, int slices);
+/* Default method of the drop-in sgemm_ (FP32 / TF32 / TF32X3 / BF16X3);
+ * env B2_SGEMM_METHOD=fp32|tf32|tf32x3|bf16x3. */
+B2_API int b2_set_sgemm_method(int method);
+
+/* ------------------------------------------------------------------------ */
+/* Drop-in Fortran-BLAS symbols                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces GEMM_DRIVER built as dgemm_ (src/gemm_driver.c:116, -DDOUBLE per
+ * Makefile:11-12) and the OpenBLAS-like dgemm_ (OpenBLAS-like_implementation/
+ * dgemm.c:484).  C <- alpha*op(A)*op(B) + beta*C. */
+B2_API void dgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+            const double *alpha, const double *a, const int *lda, const double *b,
+            const int *ldb, const double *beta, double *c, const int *ldc);
+
+/* Replaces GEMM_DRIVER built as sgemm_ (src/gemm_driver.c:116, Makefile:14-15). */
+B2_API void sgemm_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+            const float *alpha, const float *a, const int *lda, const float *b, const int *ldb,
+            const float *beta, float *c, const int *ldc);
+
+/* Replaces the upper-case serial harness symbol SGEMM_ of
+ * OpenBLAS-like_implementation/sgemm.c:579 (same contract as sgemm_). */
+B2_API void SGEMM_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+            const float *alpha, const float *a, const int *lda, const float *b, const int *ldb,
+            const float *beta, float *c, const int *ldc);
+
+/* Fortran-BLAS dtrsm_.  The reference ships the solve kernels
+ * dtrsm_solve_{ln,lt,rn,rt}_m*n* (OpenBLAS-like_implementation/dtrsm_16x4/
+ * dtrsm_kernel_16x4_skylakex.S:1863-2536, semantics in
+ * dtrsm_kernel_16x4_tester.c:66-199) that an OpenBLAS trsm driver calls; this
+ * symbol is that driver and its kernels.  side 'L': op(A) X = alpha B,
+ * side 'R': X op(A) = alpha B; B is overwritten by X. */
+B2_API void dtrsm_(const char *side, const char *uplo, const char *transa, const char *diag,
+            const int *m, const int *n, const double *alpha, const double *a, const int *lda,
+            double *b, const int *ldb);
+
+/* 3M complex GEMM (interleaved re/im; alpha, beta and matrices complex;
+ * ld in complex elements; trans 'N','T','C' conjugate-transpose,'R' conjugate).
+ * Replaces the OpenBLAS gemm3m driver + kernels
+ * zgemm3m_kernel_2x8_skylakex.c:336-351 (and the 8x4 variant :309-334) and
+ * cgemm3m_kernel_16x4_skylakex.c:415-440; all three real products and the
+ * pre/post additions run in one fused launch. */
+B2_API void zgemm3m_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+              const double *alpha, const double *a, const int *lda, const double *b,
+              const int *ldb, const double *beta, double *c, const int *ldc);
+B2_API void cgemm3m_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+              const float *alpha, const float *a, const int *lda, const float *b,
+              const int *ldb, const float *beta, float *c, const int *ldc);
+
+/* ------------------------------------------------------------------------ */
+/* Extended API (device pointers, stream-ordered, returns b2_status)         */
+/* ------------------------------------------------------------------------ */
+
+/* Same contract as dgemm_ (src/gemm_driver.c:116) on device memory.
+ * method: B2_METHOD_FP64 / _OZAKI / _AUTO / _DEFAULT; slices: Ozaki modulus
+ * count (0 = automatic).  Host pointers are rejected with B2_ERR_ARG. */
+B2_API int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha, const double *A,
+             int lda, const double *B, int ldb, double beta, double *C, int ldc, int method,
+             int slices, void *stream);
+
+/* Same contract as sgemm_ (src/gemm_driver.c:116) on device memory. */
+B2_API int b2_sgemm(char transa, char transb, int m, int n, int k, float alpha, const float *A,
+             int lda, const float *B, int ldb, float beta, float *C, int ldc, int method,
+             void *stream);
+
+/* Double-double GEMM (the accuracy yardstick): Chi + Clo ~= alpha*op(A)*op(B)
+ * + beta*C0 to ~2^-104 relative, beta semantics as dgemm_.  C0 may be NULL
+ * (treated as zero); Clo may be NULL.  Outputs are m x n with leading
+ * dimension ldo.  No counterpart in the reference: it is the oracle every
+ * result's error is stated against. */
+B2_API int b2_dgemm_dd(char transa, char transb, int m, int n, int k, double alpha, const double *A,
+                int lda, const double *B, int ldb, double beta, const double *C0, int ldc,
+                double *Chi, double *Clo, int ldo, void *stream);
+
+/* Same contract as dtrsm_ on device memory.  update_method selects the GEMM
+ * that performs the trailing updates (B2_METHOD_FP64 or B2_METHOD_OZAKI);
+ * block = diagonal block order (0 = 128). */
+B2_API int b2_dtrsm(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+             const double *A, int lda, double *B, int ldb, int update_method, int block,
+             void *stream);
+
+/* Same contracts as zgemm3m_ / cgemm3m_ on device memory. */
+B2_API int b2_zgemm3m(char transa, char transb, int m, int n, int k, const double *alpha,
+               const double *A, int lda, const double *B, int ldb, const double *beta, double *C,
+               int ldc, void *stream);
+B2_API int b2_cgemm3m(char transa, char transb, int m, int n, int k, const float *alpha,
+               const float *A, int lda, const float *B, int ldb, const float *beta, float *C,
+               int ldc, void *stream);
+
+/* Error statistics of C against a double-double reference computed on the
+ * device from the same inputs: normwise ||C - Cdd||_F / ||Cdd||_F and
+ * max_ij |C - Cdd| / max_ij |Cdd|.  Synchronous.  Allocates scratch. */
+B2_API int b2_dgemm_error(char transa, char transb, int m, int n, int k, double alpha,
+                   const double *A, int lda, const double *B, int ldb, double beta,
+                   const double *C0, const double *C, int ldc, double *normwise,
+                   double *maxelem, void *stream);
+
+/* Device-side error word: non-zero after a bounded wait inside a kernel gave
+ * up (B2_ERR_TIMEOUT).  Reading it synchronizes the library stream; clear
+ * resets it. */
+B2_API int b2_device_error(int clear);
+
+
+/* ------------------------------------------------------------------------ */
+/* Tuning hooks (replace the compile-time block sizes of dgemm_tune.h:6-15,  */
+/* sgemm_tune.h:6-15 and src/gemm_set_parameters.h:10-82)                    */
+/* ------------------------------------------------------------------------ */
+
+/* Per-thread override of the plain-FP64 kernel configuration used by every
+ * later FP64 GEMM on this thread: tile 0 = 128x128, 1 = 128x64, 2 = 64x64;
+ * mmak = DMMA K shape 4, 8 or 16; split_k >= 1.  tile < 0 clears the
+ * override (the selector decides again). */
+B2_API int b2_set_fp64_config(int tile, int mmak, int split_k);
+
+/* ------------------------------------------------------------------------ */
+/* Tracing (no counterpart in the reference, whose only instrumentation is   */
+/* the tester's clock_gettime loops, dtrsm_kernel_16x4_tester.c:267-287)     */
+/* ------------------------------------------------------------------------ */
+
+/* Kernel launches this library has issued in this process (all threads). */
+B2_API long long b2_launch_count(void);
+/* Per-thread kernel timing: when on, every launch is bracketed by CUDA events
+ * on its own stream.  b2_profile_report synchronizes those events, writes one
+ * line "name launches total_ms" per kernel into buf (NUL-terminated, at most
+ * len bytes) and clears the records; returns the number of kernels listed. */
+B2_API int b2_profile_enable(int on);
+B2_API int b2_profile_report(char *buf, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B2BLAS_H */

@@ -1,0 +1,77 @@
+"""CPU tests of the C ABI: the library loads, exports every symbol the header
+declares, and the host-side argument checks behave like BLAS xerbla without
+touching C (no GPU is needed for any of this: argument checks run before the
+library looks for a device)."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+from gemm_avx512f_b200 import _lib
+from gemm_avx512f_b200 import blas
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    declared = _lib.declared_symbols()
+    assert {"dgemm_", "sgemm_", "dtrsm_", "zgemm3m_", "cgemm3m_", "b2_dgemm"} <= set(declared)
+    missing = [s for s in declared if not hasattr(L, s)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert set(declared) <= exported
+    # nothing else leaks out of the library (internal symbols are hidden)
+    assert exported - set(declared) <= {"_init", "_fini"}
+
+
+def test_drop_in_signature_matches_reference_abi():
+    # dgemm_(const char*, const char*, const int* x3, const double*, const double*,
+    #        const int*, const double*, const int*, const double*, double*, const int*)
+    fn = _lib.lib().dgemm_
+    assert len(fn.argtypes) == 13 and fn.restype is None
+
+
+@pytest.mark.parametrize("args,info", [
+    (dict(m=-1), 3), (dict(n=-2), 4), (dict(k=-1), 5), (dict(lda=3), 8), (dict(ldb=2), 10),
+    (dict(ldc=4), 13)])
+def test_dgemm_argument_errors_leave_c_untouched(args, info):
+    m, n, k = args.get("m", 5), args.get("n", 6), args.get("k", 7)
+    lda, ldb, ldc = args.get("lda", 5), args.get("ldb", 7), args.get("ldc", 5)
+    a = np.ones((7, 7), order="F")
+    b = np.ones((7, 7), order="F")
+    c = np.full((7, 7), 3.0, order="F")
+    before = c.copy()
+    with pytest.raises(_lib.B2Error) as ei:
+        blas.dgemm("N", "N", m, n, k, 1.0, a, lda, b, ldb, 0.0, c, ldc)
+    assert ei.value.status == _lib.B2_ERR_ARG and ei.value.info == info
+    assert np.array_equal(c, before)
+
+
+def test_transposed_leading_dimension_rules():
+    a = np.ones((7, 7), order="F")
+    c = np.zeros((7, 7), order="F")
+    # transA='T': A is k x m, so lda must be >= k (=7), 5 is invalid -> info 8
+    with pytest.raises(_lib.B2Error) as ei:
+        blas.dgemm("T", "N", 5, 5, 7, 1.0, a, 5, a, 7, 0.0, c, 7)
+    assert ei.value.info == 8
+    # transB='X' (any non-N char) means transpose: B is n x k, ldb >= n (=6)
+    with pytest.raises(_lib.B2Error) as ei:
+        blas.dgemm("N", "X", 7, 6, 5, 1.0, a, 7, a, 5, 0.0, c, 7)
+    assert ei.value.info == 10
+
+
+def test_null_c_is_rejected():
+    L = _lib.lib()
+    one = C.c_double(1.0)
+    i5 = C.c_int(5)
+    L.dgemm_(b"N", b"N", C.byref(i5), C.byref(i5), C.byref(i5), C.byref(one), None,
+             C.byref(i5), None, C.byref(i5), C.byref(one), None, C.byref(i5))
+    assert blas.last_error() == (_lib.B2_ERR_ARG, 12)
+
+
+def test_status_strings():
+    L = _lib.lib()
+    for s in range(7):
+        assert L.b2_status_string(s)
