@@ -1,0 +1,422 @@
+// umma.cuh -- the sm_100a tensor-core GEMM engine (tcgen05 + TMA + TMEM).
+//
+// Computes, for every batch b < nbatch,
+//     D_b[p][q] = sum_k X_b[p][k] * Y_b[q][k]          (both operands K-major)
+// and hands each 32-column strip of a 128 x BN accumulator tile to an
+// epilogue functor.  This is the B200 replacement of the reference's whole
+// GEMM machinery: the OpenMP N split and thread-0 packing of
+// src/gemm_driver.c:136-188 become a persistent grid over output tiles, the
+// packing of src/gemm_copy.c becomes TMA loads into 128B-swizzled shared
+// memory, and the 24x8 FMA register tile of src/kernel/gemm_kernel.S becomes
+// 128 x BN x 32-byte tcgen05.mma instructions accumulating in TMEM.
+//
+// Roles (192 threads, one CTA per SM):
+//   warp 0      TMA producer: fills a STAGES-deep ring of (X, Y) K-blocks.
+//   warp 1      TMEM owner + MMA issuer (one elected lane).
+//   warps 2..5  epilogue: tcgen05.ld of their 32-lane quarter of the
+//               accumulator, then the functor.
+// TMEM holds two accumulators (2 x BN columns) so the epilogue of tile i
+// overlaps the MMAs of tile i+1.
+//
+// Every mbarrier wait is bounded (B2_WAIT_NS of wall time from %globaltimer);
+// on expiry the waiter records B2_ERR_TIMEOUT in the device error word and
+// raises a shared abort flag, every role drains and leaves its loop, the
+// in-flight copies and MMAs are waited for (again bounded), TMEM is freed and
+// the kernel returns.  Nothing traps.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "b2_internal.cuh"
+#include "b2_profile.cuh"
+
+namespace b2 {
+namespace umma {
+
+enum Kind { KIND_I8 = 0, KIND_BF16 = 1, KIND_TF32 = 2 };
+
+constexpr int BM = 128;            // accumulator lanes (X rows) per tile
+constexpr int KBLOCK_BYTES = 128;  // one 128B swizzle atom along K per stage
+constexpr int THREADS = 192;
+constexpr uint64_t B2_WAIT_NS = 2000000000ull;  // 2 s per wait: far above any legal wait
+
+__host__ __device__ constexpr int elem_bytes(int kind) { return kind == KIND_I8 ? 1 : kind == KIND_BF16 ? 2 : 4; }
+
+// Instruction descriptor (PTX ISA tcgen05 "instruction descriptor" for
+// .kind::f16 / .kind::tf32 / .kind::i8): D format at [4,6), A/B formats at
+// [7,10)/[10,13), K-major A and B (bits 15/16 clear), N>>3 at [17,23),
+// M>>4 at [24,29).
+__host__ __device__ constexpr uint32_t make_idesc(int kind, int m, int n) {
+  const uint32_t dfmt = kind == KIND_I8 ? 2u : 1u;       // S32 : F32
+  const uint32_t abfmt = kind == KIND_I8 ? 1u             // signed 8-bit
+                         : kind == KIND_BF16 ? 1u          // BF16
+                                             : 2u;         // TF32
+  return (dfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+// ----------------------------------------------------------- PTX helpers --
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait.  Returns false if the wait was abandoned (timeout here or an
+// abort raised by another role); the first timeout records the error.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                          int *derr) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = gtimer();
+  for (uint32_t it = 1;; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 255u) == 0) {
+      if (*abort_flag) return false;
+      if (gtimer() - t0 > B2_WAIT_NS) {
+        *abort_flag = 1;
+        atomicCAS(derr, 0, (int)B2_ERR_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)map) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+template <int KIND>
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  if constexpr (KIND == KIND_I8) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else if constexpr (KIND == KIND_BF16) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  }
+}
+
+// Shared-memory matrix descriptor for a K-major operand tile stored as rows of
+// 128 bytes with the 128B swizzle (the layout TMA writes with
+// CU_TENSOR_MAP_SWIZZLE_128B): start address >> 4 at [0,14), leading byte
+// offset (unused for this layout) = 1 at [16,30), stride byte offset = 1024 B
+// (8 rows x 128 B) >> 4 at [32,46), descriptor version 1 at [46,48), base
+// offset 0 (tile bases are 1024-B aligned), swizzle mode 2 = 128B at [61,64).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+// Wait for tcgen05.ld; the registers are threaded through so no use of them
+// can be scheduled above the wait.
+__device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[32]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
+}
+
+// ---------------------------------------------------------------- kernel --
+struct Problem {
+  int P, Q;        // rows of X and of Y (output tile space P x Q)
+  int kblocks;     // K extent in 128-byte blocks
+  int nbatch;      // independent products (3-D tensor maps, batch = outer coordinate)
+  int tiles_p, tiles_q;
+  int group;       // tile rasterisation: GROUP rows of P tiles share a sweep over Q
+  int *derr;       // device error word
+};
+
+template <int BN, int STAGES>
+struct SmemLayout {
+  static constexpr int X_BYTES = BM * KBLOCK_BYTES;
+  static constexpr int Y_BYTES = BN * KBLOCK_BYTES;
+  static constexpr int STAGE_BYTES = X_BYTES + Y_BYTES;
+  static constexpr int BAR_OFF = STAGES * STAGE_BYTES;
+  // full[S], empty[S], tfull[2], tempty[2], drain, then tmem address + abort flag
+  static constexpr int BAR_BYTES = (2 * STAGES + 5) * 8;
+  static constexpr int TOTAL = BAR_OFF + BAR_BYTES + 16 + 1024;  // + alignment slack
+};
+
+__device__ __forceinline__ void tile_coords(const Problem &pr, int t, int &b, int &tp, int &tq) {
+  const int per_batch = pr.tiles_p * pr.tiles_q;
+  b = t / per_batch;
+  const int r = t - b * per_batch;
+  const int gsz = pr.group * pr.tiles_q;
+  const int g = r / gsz;
+  const int first_p = g * pr.group;
+  const int gp = min(pr.group, pr.tiles_p - first_p);
+  const int rr = r - g * gsz;
+  tp = first_p + rr % gp;
+  tq = rr / gp;
+}
+
+template <int KIND, int BN, int STAGES, class Epi>
+__global__ void __launch_bounds__(THREADS, 1)
+    umma_gemm_kernel(const __grid_constant__ CUtensorMap tmX,
+                     const __grid_constant__ CUtensorMap tmY, const Problem pr, const Epi epi) {
+  using L = SmemLayout<BN, STAGES>;
+  static_assert(2 * BN <= 512, "two accumulators must fit in TMEM");
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *gbase = smem_raw + (base - raw);
+  const uint32_t bar0 = base + L::BAR_OFF;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+  auto tfull_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };
+  auto tempty_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };
+  const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + L::BAR_OFF + L::BAR_BYTES);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(gbase + L::BAR_OFF + L::BAR_BYTES + 8);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int total_tiles = pr.tiles_p * pr.tiles_q * pr.nbatch;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull_bar(a), 1);
+      mbar_init(tempty_bar(a), 4);  // one arrival per epilogue warp
+    }
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    prefetch_tmap(&tmX);
+    prefetch_tmap(&tmY);
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(2 * BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      constexpr int EB = 0;  // silence unused warnings in some instantiations
+      (void)EB;
+      const int kcoord = KBLOCK_BYTES / elem_bytes(KIND);
+      int stage = 0;
+      uint32_t phase = 0;
+      long issued = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+        int b, tp, tq;
+        tile_coords(pr, t, b, tp, tq);
+        for (int kb = 0; kb < pr.kblocks; ++kb) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, pr.derr)) { ok = false; break; }
+          const uint32_t sx = base + stage * L::STAGE_BYTES;
+          const uint32_t sy = sx + L::X_BYTES;
+          mbar_expect_tx(full_bar(stage), L::STAGE_BYTES);
+          tma_load_3d(sx, &tmX, full_bar(stage), kb * kcoord, tp * BM, b);
+          tma_load_3d(sy, &tmY, full_bar(stage), kb * kcoord, tq * BN, b);
+          ++issued;
+          if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+        }
+      }
+      if (!ok) {
+        // Abandoned: wait (bounded) until every issued copy has landed so no
+        // TMA writes into shared memory after this CTA retires.
+        long first = issued - STAGES > 0 ? issued - STAGES : 0;
+        for (long i = first; i < issued; ++i) {
+          const int s = (int)(i % STAGES);
+          const uint32_t ph = (uint32_t)((i / STAGES) & 1);
+          const uint64_t t0 = gtimer();
+          while (!mbar_try_wait(full_bar(s), ph) && gtimer() - t0 < B2_WAIT_NS) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // -------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      constexpr uint32_t idesc = make_idesc(KIND, BM, BN);
+      int stage = 0;
+      uint32_t phase = 0;
+      int it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+        const int acc = it & 1;
+        const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+        if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag, pr.derr)) { ok = false; break; }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+        for (int kb = 0; kb < pr.kblocks; ++kb) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag, pr.derr)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t sx = base + stage * L::STAGE_BYTES;
+          const uint32_t sy = sx + L::X_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < KBLOCK_BYTES / 32; ++kk) {
+            tc_mma<KIND>(d_tmem, sw128_desc(sx + kk * 32), sw128_desc(sy + kk * 32), idesc,
+                         (kb | kk) ? 1u : 0u);
+          }
+          tc_commit(empty_bar(stage));  // frees the stage once these MMAs have read it
+          if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+        }
+        if (!ok) break;
+        tc_commit(tfull_bar(acc));
+      }
+      // All MMAs issued so far complete before the drain barrier flips.
+      tc_commit(drain_bar);
+      const uint64_t t0 = gtimer();
+      while (!mbar_try_wait(drain_bar, 0) && gtimer() - t0 < B2_WAIT_NS) {
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int quarter = warp & 3;  // TMEM lanes this warp may access
+    int it = 0;
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+      int b, tp, tq;
+      tile_coords(pr, t, b, tp, tq);
+      const int acc = it & 1;
+      const bool ok = mbar_wait(tfull_bar(acc), (uint32_t)((it >> 1) & 1), abort_flag, pr.derr);
+      if (!__all_sync(0xffffffffu, ok)) break;  // keep the warp converged for tcgen05.ld
+      tc_fence_after();
+      const int p = tp * BM + quarter * 32 + lane;
+      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+      for (int c = 0; c < BN / 32; ++c) {
+        uint32_t v[32];
+        tmem_ld32(taddr + (uint32_t)(c * 32), v);
+        tmem_ld_wait(v);
+        epi(b, p, tq * BN + c * 32, v);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty_bar(acc));
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                 "r"(2 * BN));
+  }
+}
+
+// ------------------------------------------------------------------ host --
+// 3-D tensor map over `nbatch` planes of `rows` x `kelems` K-major elements
+// (row pitch `row_bytes`, plane pitch `plane_bytes`, both multiples of 16),
+// box = 128 B of K x box_rows rows x 1 plane, 128B swizzle, OOB zero fill.
+int make_kmajor_map(CUtensorMap *map, int kind, const void *base, long long kelems, long long rows,
+                    long long nbatch, long long row_bytes, long long plane_bytes, int box_rows);
+
+template <int KIND, int BN, int STAGES, class Epi>
+int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
+           int nbatch, const Epi &epi, int sm_count, int *derr, cudaStream_t s,
+           const char *prof_name, int max_ctas = 0) {
+  using L = SmemLayout<BN, STAGES>;
+  Problem pr;
+  pr.P = P;
+  pr.Q = Q;
+  pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
+  pr.nbatch = nbatch;
+  pr.tiles_p = (P + BM - 1) / BM;
+  pr.tiles_q = (Q + BN - 1) / BN;
+  pr.group = 8;
+  pr.derr = derr;
+  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch;
+  if (total <= 0) return B2_OK;
+  int grid = (int)(total < sm_count ? total : sm_count);
+  if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+  auto kern = umma_gemm_kernel<KIND, BN, STAGES, Epi>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
+  if (e != cudaSuccess) return cuda_fail(e, "umma smem attribute");
+  B2_PROF(prof_name, s);
+  kern<<<grid, THREADS, L::TOTAL, s>>>(tmX, tmY, pr, epi);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, prof_name);
+  return B2_OK;
+}
+
+}  // namespace umma
+}  // namespace b2

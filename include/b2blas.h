@@ -126,6 +126,10 @@ B2_API int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha,
              int lda, const double *B, int ldb, double beta, double *C, int ldc, int method,
              int slices, void *stream);
 
+/* Plan of the last Ozaki DGEMM on this thread: out[0] = modulus (slice)
+ * count, out[1] = number of K chunks (K is cut at 65536 per exact INT32 pass). */
+B2_API int b2_ozaki_last_plan(int *out, int n);
+
 /* Same contract as sgemm_ (src/gemm_driver.c:116) on device memory. */
 B2_API int b2_sgemm(char transa, char transb, int m, int n, int k, float alpha, const float *A,
              int lda, const float *B, int ldb, float beta, float *C, int ldc, int method,
