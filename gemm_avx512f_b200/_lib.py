@@ -82,6 +82,8 @@ def lib() -> C.CDLL:
     L.b2_cgemm3m.argtypes = [ch, ch, i, i, i, p, p, i, p, i, p, p, i, p]
     L.b2_dgemm_error.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, p, i, pd, pd, p]
     L.b2_device_error.argtypes = [i]
+    L.b2_dgemm_ozaki_noalloc.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, p]
+    L.b2_dgemm_ozaki_noalloc.restype = i
     L.b2_set_fp64_config.argtypes = [i, i, i]
     L.b2_set_fp64_config.restype = i
     L.b2_launch_count.restype = C.c_longlong

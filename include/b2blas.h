@@ -130,6 +130,24 @@ B2_API int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha,
  * count, out[1] = number of K chunks (K is cut at 65536 per exact INT32 pass). */
 B2_API int b2_ozaki_last_plan(int *out, int n);
 
+/* Allocation-free INT8 Ozaki DGEMM.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory at call time (code running
+ * during CUDA graph capture, real-time loops that must stay out of the
+ * allocator, processes whose device memory is reserved up front).  Same
+ * contract and result as b2_dgemm(..., B2_METHOD_OZAKI, slices, stream) on
+ * device pointers, but all scratch lives in one static device array of
+ * B2_NOALLOC_SCRATCH_BYTES per device, reserved when the library loads and
+ * held until exit; the call never allocates or frees.  Problems whose scratch
+ * exceeds that maximum (about 1200^3 at 15 moduli; K <= 65536) return
+ * B2_ERR_ARG.  Every call shares the array, so calls that overlap on the GPU
+ * race and must be serialised by the caller.  The first call on a device
+ * resolves the array's device address; make it before any stream capture.
+ * stream NULL = the legacy default stream. */
+#define B2_NOALLOC_SCRATCH_BYTES (64ull << 20)
+B2_API int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, int k, double alpha,
+                                  const double *A, int lda, const double *B, int ldb,
+                                  double beta, double *C, int ldc, int slices, void *stream);
+
 /* Same contract as sgemm_ (src/gemm_driver.c:116) on device memory. */
 B2_API int b2_sgemm(char transa, char transb, int m, int n, int k, float alpha, const float *A,
              int lda, const float *B, int ldb, float beta, float *C, int ldc, int method,
