@@ -52,6 +52,8 @@ struct CrtTable {
   int H;                 // scaling target: 2-norms scaled to <= 2^H
   long long W[OZ_MAX][3];  // CRT weights, 42-bit limbs (low first)
   long long Pl[3];       // P in 42-bit limbs
+  double Wd[OZ_MAX][4];  // CRT weights in 32-bit limbs
+  double Pd[4];          // P in 32-bit limbs
   double invP;
   double log2P;
 };
@@ -62,6 +64,10 @@ __constant__ double c_invd[OZ_MAX];
 __constant__ unsigned c_k16[OZ_MAX];  // 2^16 mod m
 __constant__ unsigned c_k32[OZ_MAX];  // 2^32 mod m
 __constant__ unsigned c_k48[OZ_MAX];  // 2^48 mod m
+__constant__ unsigned c_off[OZ_MAX];  // m - (2^62 mod m): undoes the +2^62 offset
+__constant__ unsigned c_magic[OZ_MAX];  // floor(2^32 / m) + 1 (Barrett)
+__constant__ double c_Wd[OZ_MAX][4];  // CRT weights in 32-bit limbs (low first)
+__constant__ double c_Pd[4];          // P in 32-bit limbs
 __constant__ long long c_W[OZ_MAX][3];
 __constant__ long long c_P[3];
 __constant__ double c_invP;
@@ -90,7 +96,9 @@ CrtTable make_table(int s) {
     t.W[i][0] = (long long)(W & (u128)(LIMB - 1));
     t.W[i][1] = (long long)((W >> 42) & (u128)(LIMB - 1));
     t.W[i][2] = (long long)(W >> 84);
+    for (int l = 0; l < 4; ++l) t.Wd[i][l] = (double)(unsigned long long)((W >> (32 * l)) & 0xFFFFFFFFu);
   }
+  for (int l = 0; l < 4; ++l) t.Pd[l] = (double)(unsigned long long)((P >> (32 * l)) & 0xFFFFFFFFu);
   t.Pl[0] = (long long)(P & (u128)(LIMB - 1));
   t.Pl[1] = (long long)((P >> 42) & (u128)(LIMB - 1));
   t.Pl[2] = (long long)(P >> 84);
@@ -99,7 +107,68 @@ CrtTable make_table(int s) {
 }
 
 // ------------------------------------------------------- norm exponents --
-// Running sum of squares with a power-of-two scale: value = s * 4^e.
+// Fast partial pass: plain sum of squares and max |x| per (row, K chunk).
+// Exact enough whenever the row's max |x| lies in [2^-480, 2^480]: no square
+// comes near overflow, and squares that underflow (|x| < 2^-511) add less
+// than K 2^-1022, negligible against max^2 >= 2^-960.  Rows outside that
+// range, and rows holding Inf/NaN (their sum turns non-finite), are redone
+// by the finalize kernel with a power-of-two-scaled sum.
+template <bool ROWCONT>
+__global__ void norm_partial_kernel(const double *__restrict__ X, long long sr, long long sk,
+                                    int R, int K, int kchunk, double *__restrict__ pmax,
+                                    double *__restrict__ pssq) {
+  const int chunk = blockIdx.y;
+  const int k0 = chunk * kchunk, k1 = min(K, k0 + kchunk);
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  int r;
+  if (ROWCONT) {
+    r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    const double *p = X + r;
+    int k = k0;
+    for (; k + 3 < k1; k += 4) {
+      const double a0 = __ldg(p + (long long)k * sk), a1 = __ldg(p + (long long)(k + 1) * sk);
+      const double a2 = __ldg(p + (long long)(k + 2) * sk), a3 = __ldg(p + (long long)(k + 3) * sk);
+      s0 = fma(a0, a0, s0); s1 = fma(a1, a1, s1); s2 = fma(a2, a2, s2); s3 = fma(a3, a3, s3);
+      m0 = fmax(m0, fabs(a0)); m1 = fmax(m1, fabs(a1)); m2 = fmax(m2, fabs(a2)); m3 = fmax(m3, fabs(a3));
+    }
+    for (; k < k1; ++k) {
+      const double a0 = __ldg(p + (long long)k * sk);
+      s0 = fma(a0, a0, s0);
+      m0 = fmax(m0, fabs(a0));
+    }
+  } else {
+    const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
+    r = blockIdx.x * warps + (threadIdx.x >> 5);
+    if (r >= R) return;
+    const double *p = X + (long long)r * sr;
+    int k = k0 + lane;
+    for (; k + 96 < k1; k += 128) {
+      const double a0 = __ldg(p + k), a1 = __ldg(p + k + 32), a2 = __ldg(p + k + 64),
+                   a3 = __ldg(p + k + 96);
+      s0 = fma(a0, a0, s0); s1 = fma(a1, a1, s1); s2 = fma(a2, a2, s2); s3 = fma(a3, a3, s3);
+      m0 = fmax(m0, fabs(a0)); m1 = fmax(m1, fabs(a1)); m2 = fmax(m2, fabs(a2)); m3 = fmax(m3, fabs(a3));
+    }
+    for (; k < k1; k += 32) {
+      const double a0 = __ldg(p + k);
+      s0 = fma(a0, a0, s0);
+      m0 = fmax(m0, fabs(a0));
+    }
+  }
+  double s = (s0 + s1) + (s2 + s3), mx = fmax(fmax(m0, m1), fmax(m2, m3));
+  if (!ROWCONT) {
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_down_sync(0xffffffffu, s, o);
+      mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) != 0) return;
+  }
+  pmax[(long long)chunk * R + r] = mx;
+  pssq[(long long)chunk * R + r] = s;
+}
+
+// Scaled sum of squares for the rare rows outside the fast range:
+// value = s * 4^e with every term scaled by the running power of two.
 struct Ssq {
   int e;
   double s;
@@ -116,95 +185,61 @@ __device__ __forceinline__ void ssq_add(Ssq &a, double x) {
   const double y = scalbn(x, -a.e);
   a.s = fma(y, y, a.s);
 }
-__device__ __forceinline__ void ssq_merge(Ssq &a, int e, double s, int bad) {
-  a.bad |= bad;
-  if (s == 0.0) return;
-  if (e > a.e) {
-    a.s = scalbn(a.s, 2 * (a.e - e));
-    a.e = e;
-    a.s += s;
-  } else {
-    a.s += scalbn(s, 2 * (e - a.e));
-  }
-}
 
-// Partial sums over K chunks for the R "rows" of an operand viewed as R x K
-// with element (r, k) at X[r*sr + k*sk].  ROWCONT: sr == 1 (thread per row);
-// else sk == 1 (warp per row, lanes along k).  Output part[chunk*R + r].
-template <bool ROWCONT>
-__global__ void norm_partial_kernel(const double *__restrict__ X, long long sr, long long sk,
-                                    int R, int K, int kchunk, int *__restrict__ pe,
-                                    double *__restrict__ ps, int *__restrict__ pbad) {
-  const int chunk = blockIdx.y;
-  const int k0 = chunk * kchunk, k1 = min(K, k0 + kchunk);
-  if (ROWCONT) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= R) return;
-    Ssq a{-2000, 0.0, 0};
-    const double *p = X + r;
-    for (int k = k0; k < k1; ++k) ssq_add(a, __ldg(p + (long long)k * sk));
-    pe[(long long)chunk * R + r] = a.e;
-    ps[(long long)chunk * R + r] = a.s;
-    pbad[(long long)chunk * R + r] = a.bad;
-  } else {
-    const int warps = blockDim.x >> 5;
-    const int r = blockIdx.x * warps + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (r >= R) return;
-    Ssq a{-2000, 0.0, 0};
-    const double *p = X + (long long)r * sr;
-    for (int k = k0 + lane; k < k1; k += 32) ssq_add(a, __ldg(p + k));
-    for (int o = 16; o > 0; o >>= 1) {
-      const int e = __shfl_down_sync(0xffffffffu, a.e, o);
-      const double s = __shfl_down_sync(0xffffffffu, a.s, o);
-      const int b = __shfl_down_sync(0xffffffffu, a.bad, o);
-      ssq_merge(a, e, s, b);
-    }
-    if (lane == 0) {
-      pe[(long long)chunk * R + r] = a.e;
-      ps[(long long)chunk * R + r] = a.s;
-      pbad[(long long)chunk * R + r] = a.bad;
-    }
-  }
-}
-
-// Combine the chunks: sigma_r = H - ceil(log2 ||x_r||_2), NONFINITE if the row
-// holds Inf/NaN, 0 for an all-zero row.
-__global__ void norm_finalize_kernel(const int *__restrict__ pe, const double *__restrict__ ps,
-                                     const int *__restrict__ pbad, int R, int chunks, int H,
-                                     int *__restrict__ sigma) {
+// sigma_r = H - ceil(log2 ||x_r||_2); NONFINITE if the row holds Inf/NaN;
+// 0 for an all-zero row.
+__global__ void norm_finalize_kernel(const double *__restrict__ pmax,
+                                     const double *__restrict__ pssq, int R, int chunks, int H,
+                                     int *__restrict__ sigma, const double *__restrict__ X,
+                                     long long sr, long long sk, int K) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= R) return;
-  Ssq a{-2000, 0.0, 0};
-  for (int c = 0; c < chunks; ++c)
-    ssq_merge(a, pe[(long long)c * R + r], ps[(long long)c * R + r], pbad[(long long)c * R + r]);
-  if (a.bad) { sigma[r] = NONFINITE; return; }
-  if (a.s == 0.0) { sigma[r] = 0; return; }
-  int g;
-  frexp(a.s * (1.0 + 0x1p-30), &g);  // s (1+eps) < 2^g, so ||x|| < 2^(e + ceil(g/2))
-  const int enorm = a.e + ((g + 1) >> 1);
-  sigma[r] = H - enorm;
+  double mx = 0.0, ss = 0.0;
+  for (int c = 0; c < chunks; ++c) {
+    mx = fmax(mx, pmax[(long long)c * R + r]);
+    ss += pssq[(long long)c * R + r];
+  }
+  if (mx == 0.0 && ss == 0.0) { sigma[r] = 0; return; }
+  int g, e = 0;
+  if (isfinite(ss) && mx >= 0x1p-480 && mx <= 0x1p480) {
+    frexp(ss * (1.0 + 0x1p-30), &g);  // ss (1+eps) < 2^g, so ||x|| < 2^ceil(g/2)
+  } else {
+    Ssq a{-2000, 0.0, 0};
+    const double *p = X + (long long)r * sr;
+    for (int k = 0; k < K; ++k) ssq_add(a, p[(long long)k * sk]);
+    if (a.bad) { sigma[r] = NONFINITE; return; }
+    if (a.s == 0.0) { sigma[r] = 0; return; }
+    frexp(a.s * (1.0 + 0x1p-30), &g);
+    e = a.e;
+  }
+  sigma[r] = H - (e + ((g + 1) >> 1));
 }
 
 // --------------------------------------------------------- residue slices --
-// |x| = c3 2^48 + c2 2^32 + c1 2^16 + c0 (16-bit limbs, c3 < 2^14): the limb
-// sum s < 2^26 keeps the float quotient estimate within +-1 of floor(s/m)
-// (relative error <= 2^-22, so absolute error <= 2^26/193 * 2^-22 < 0.1).
+// x + 2^62 >= 0 is split into 16-bit limbs c3..c0 (c3 < 2^15); the limb sum
+// with the precomputed powers 2^16j mod m, plus (m - 2^62 mod m) to undo the
+// offset, stays below 2^26 + 256.  Barrett with magic = floor(2^32/m) + 1
+// over-estimates the quotient by at most s/2^32 < 1/64, so one correction
+// brings s - q m into [0, m); the symmetric representative follows.
 __device__ __forceinline__ int sym_residue(unsigned c0, unsigned c1, unsigned c2, unsigned c3,
                                            int i) {
   const int m = c_mod[i];
-  const unsigned s = c0 + c1 * c_k16[i] + c2 * c_k32[i] + c3 * c_k48[i];  // < 2^26
-  const int q = (int)(__uint2float_rz(s) * c_invf[i]);
-  int r = (int)s - q * m;  // within one modulus of [0, m)
+  const unsigned s = c0 + c1 * c_k16[i] + c2 * c_k32[i] + c3 * c_k48[i] + c_off[i];
+  const unsigned q = __umulhi(s, c_magic[i]);
+  int r = (int)(s - q * (unsigned)m);
   r += (r < 0) ? m : 0;
-  r -= (r >= m) ? m : 0;
-  r -= (r > ((m - 1) >> 1)) ? m : 0;  // symmetric representative
+  r -= (r > ((m - 1) >> 1)) ? m : 0;
   return r;
+}
+
+__device__ __forceinline__ double pow2(int e) {  // e in [-1022, 1023]
+  return __longlong_as_double((long long)(e + 1023) << 52);
 }
 
 // Operand viewed as R x K (element (r,k) at X[r*sr + k*sk]); writes s planes
 // out[i][r][k] (row pitch kp bytes, plane pitch plane bytes) of the symmetric
-// residues of trunc(x * 2^sigma_r).  Tile: 32 rows x 64 k, 256 threads.
+// residues of trunc(x * 2^sigma_r).  Tile: 32 rows x 64 k, 256 threads, each
+// thread 8 consecutive k of one row.
 template <bool ROWCONT>
 __global__ void __launch_bounds__(256)
     slice_kernel(const double *__restrict__ X, long long sr, long long sk, int R, int K,
@@ -227,16 +262,16 @@ __global__ void __launch_bounds__(256)
   const int rr = tid >> 3, kg = (tid & 7) * 8;
   const int r = r0 + rr;
   if (r >= R || k0 + kg >= K) return;
-  int sg = sigma[r];
+  const int sg = sigma[r];
   const bool dead = (sg == NONFINITE);
+  // 2^sigma as two in-range factors (sigma in [H-1024, H+1074])
+  const int e1 = dead ? 0 : (sg > 1000 ? 1000 : (sg < -1000 ? -1000 : sg));
+  const double f1 = pow2(e1), f2 = pow2(dead ? 0 : sg - e1);
   unsigned c0[8], c1[8], c2[8], c3[8];
-  bool neg[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
-    const double v = dead ? 0.0 : scalbn(tile[rr][kg + j], sg);
-    const long long x = __double2ll_rz(v);
-    neg[j] = x < 0;
-    const unsigned long long u = (unsigned long long)(x < 0 ? -x : x);
+    const double v = dead ? 0.0 : (tile[rr][kg + j] * f1) * f2;
+    const unsigned long long u = (unsigned long long)(__double2ll_rz(v) + (1ll << 62));
     c0[j] = (unsigned)(u & 0xFFFFull);
     c1[j] = (unsigned)((u >> 16) & 0xFFFFull);
     c2[j] = (unsigned)((u >> 32) & 0xFFFFull);
@@ -247,9 +282,7 @@ __global__ void __launch_bounds__(256)
     unsigned lo = 0, hi = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      int rv = sym_residue(c0[j], c1[j], c2[j], c3[j], i);
-      rv = neg[j] ? -rv : rv;
-      const unsigned b = (unsigned)(rv & 0xFF);
+      const unsigned b = (unsigned)(sym_residue(c0[j], c1[j], c2[j], c3[j], i) & 0xFF);
       if (j < 4) lo |= b << (8 * j); else hi |= b << (8 * (j - 4));
     }
     int8_t *dst = out + (long long)i * plane + (long long)r * kp + k0 + kg;
@@ -309,56 +342,86 @@ struct ResidueEpi {
 };
 
 // ---------------------------------------------------------- reconstruction --
-__device__ __forceinline__ double i128_to_double(__int128 v) {
-  const long long hi = (long long)(v >> 64);
-  const unsigned long long lo = (unsigned long long)v;
+// (hi * 2^64 + lo) -> double, one rounding when the value fits in 64 bits,
+// otherwise at most 1.5 ulp.
+__device__ __forceinline__ double i128_to_double(long long hi, unsigned long long lo) {
   if ((hi == 0 && (long long)lo >= 0) || (hi == -1 && (long long)lo < 0))
     return (double)(long long)lo;
   return fma((double)hi, 0x1p64, (double)lo);
 }
 
-// C(m,n) = alpha * C'(m,n) 2^-(sigma_m + tau_n) + beta C(m,n), C' from the s
-// residues by CRT.  Rows/columns flagged NONFINITE use a direct FP64 dot product.
+__device__ __forceinline__ double byte_to_double(unsigned b) {  // exact, no conversion unit
+  return __hiloint2double(0x43300000, (int)b) - 4503599627370496.0;
+}
+
+// C(m,n) = alpha * C'(m,n) 2^-(sigma_m + tau_n) + beta C(m,n).  C' is the value
+// in (-P/2, P/2) with the s residues: S = sum_i r_i W_i is accumulated exactly
+// in four 32-bit limbs held in doubles (r_i W_il < 2^40, sums < 2^44), the
+// quotient q = round(S/P) comes from one double estimate (|C'| <= P/4 keeps it
+// exact), S - qP is exact per limb, and the carries are settled in 64-bit
+// integers.  Each thread handles 4 consecutive rows m of one column n.
+// Rows/columns flagged NONFINITE use a direct FP64 dot product.
 __global__ void __launch_bounds__(256)
     reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr, int s, int M,
                        int N, const int *__restrict__ sigA, const int *__restrict__ tauB,
                        double alpha, double beta, double *__restrict__ C, int ldc,
                        const double *__restrict__ A, long long asr, long long ask,
                        const double *__restrict__ B, long long bsk, long long bsc, int K) {
-  const long long total = (long long)M * N;
+  const int M4 = (M + 3) >> 2;
+  const long long total = (long long)M4 * N;
   for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
        idx += (long long)gridDim.x * blockDim.x) {
-    const int m = (int)(idx % M), n = (int)(idx / M);
-    const int sg = sigA[m], tg = tauB[n];
-    double val;
-    if (sg == NONFINITE || tg == NONFINITE) {
-      double acc = 0.0;
-      for (int k = 0; k < K; ++k) acc = fma(A[m * asr + k * ask], B[k * bsk + n * bsc], acc);
-      val = acc;
-    } else {
-      long long S0 = 0, S1 = 0, S2 = 0;
-      const uint8_t *rp = R + (long long)n * ldr + m;
-      for (int i = 0; i < s; ++i) {
-        const long long r = rp[(long long)i * plane];
-        S0 += r * c_W[i][0];
-        S1 += r * c_W[i][1];
-        S2 += r * c_W[i][2];
+    const int m0 = (int)(idx % M4) * 4, n = (int)(idx / M4);
+    double S[4][4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+#pragma unroll
+      for (int l = 0; l < 4; ++l) S[e][l] = 0.0;
+    const uint8_t *rp = R + (long long)n * ldr + m0;
+    for (int i = 0; i < s; ++i) {
+      const unsigned w4 = *reinterpret_cast<const unsigned *>(rp + (long long)i * plane);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double rd = byte_to_double((w4 >> (8 * e)) & 0xFFu);
+#pragma unroll
+        for (int l = 0; l < 4; ++l) S[e][l] = fma(rd, c_Wd[i][l], S[e][l]);
       }
-      const double Sd = fma((double)S2, 0x1p84, fma((double)S1, 0x1p42, (double)S0));
-      const long long q = __double2ll_rn(Sd * c_invP);
-      long long X0 = S0 - q * c_P[0], X1 = S1 - q * c_P[1], X2 = S2 - q * c_P[2];
-      long long cy = X0 >> 42;
-      X0 -= cy << 42;
-      X1 += cy;
-      cy = X1 >> 42;
-      X1 -= cy << 42;
-      X2 += cy;
-      const __int128 v = (__int128)X2 * ((__int128)1 << 84) + (__int128)X1 * ((__int128)1 << 42) +
-                          (__int128)X0;
-      val = scalbn(i128_to_double(v), -(sg + tg));
     }
-    double *cp = C + (long long)n * ldc + m;
-    *cp = (beta == 1.0) ? fma(alpha, val, *cp) : fma(alpha, val, beta * *cp);
+    const int tg = tauB[n];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int m = m0 + e;
+      if (m >= M) break;
+      const int sg = sigA[m];
+      double val;
+      if (sg == NONFINITE || tg == NONFINITE) {
+        double acc = 0.0;
+        for (int k = 0; k < K; ++k) acc = fma(A[m * asr + k * ask], B[k * bsk + n * bsc], acc);
+        val = acc;
+      } else {
+        const double Sd =
+            fma(S[e][3], 0x1p96, fma(S[e][2], 0x1p64, fma(S[e][1], 0x1p32, S[e][0])));
+        const double q = rint(Sd * c_invP);
+        long long X0 = __double2ll_rn(fma(-q, c_Pd[0], S[e][0]));
+        long long X1 = __double2ll_rn(fma(-q, c_Pd[1], S[e][1]));
+        long long X2 = __double2ll_rn(fma(-q, c_Pd[2], S[e][2]));
+        long long X3 = __double2ll_rn(fma(-q, c_Pd[3], S[e][3]));
+        long long cy = X0 >> 32;
+        X0 -= cy << 32;
+        X1 += cy;
+        cy = X1 >> 32;
+        X1 -= cy << 32;
+        X2 += cy;
+        cy = X2 >> 32;
+        X2 -= cy << 32;
+        X3 += cy;
+        const unsigned long long lo = ((unsigned long long)X1 << 32) | (unsigned long long)X0;
+        const long long hi = X3 * 4294967296ll + X2;
+        val = scalbn(i128_to_double(hi, lo), -(sg + tg));
+      }
+      double *cp = C + (long long)n * ldc + m;
+      *cp = (beta == 1.0) ? fma(alpha, val, *cp) : fma(alpha, val, beta * *cp);
+    }
   }
 }
 
@@ -375,7 +438,7 @@ int upload_table(int s, int dev, cudaStream_t st) {
   int mod[OZ_MAX];
   float invf[OZ_MAX];
   double invd[OZ_MAX];
-  unsigned k16[OZ_MAX], k32[OZ_MAX], k48[OZ_MAX];
+  unsigned k16[OZ_MAX], k32[OZ_MAX], k48[OZ_MAX], off[OZ_MAX], magic[OZ_MAX];
   for (int i = 0; i < OZ_MAX; ++i) {
     mod[i] = kModuli[i];
     invf[i] = 1.0f / (float)kModuli[i];
@@ -383,6 +446,8 @@ int upload_table(int s, int dev, cudaStream_t st) {
     k16[i] = (unsigned)((1ull << 16) % (unsigned long long)kModuli[i]);
     k32[i] = (unsigned)((1ull << 32) % (unsigned long long)kModuli[i]);
     k48[i] = (unsigned)((1ull << 48) % (unsigned long long)kModuli[i]);
+    off[i] = (unsigned)(kModuli[i] - (int)((1ull << 62) % (unsigned long long)kModuli[i]));
+    magic[i] = (unsigned)((1ull << 32) / (unsigned long long)kModuli[i] + 1);
   }
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_mod, mod, sizeof(mod), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invf, invf, sizeof(invf), 0, cudaMemcpyHostToDevice, st));
@@ -390,6 +455,10 @@ int upload_table(int s, int dev, cudaStream_t st) {
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k16, k16, sizeof(k16), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k32, k32, sizeof(k32), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k48, k48, sizeof(k48), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_off, off, sizeof(off), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_magic, magic, sizeof(magic), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Wd, t.Wd, sizeof(t.Wd), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Pd, t.Pd, sizeof(t.Pd), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_W, t.W, sizeof(t.W), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_P, t.Pl, sizeof(t.Pl), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invP, &t.invP, sizeof(double), 0, cudaMemcpyHostToDevice, st));
@@ -408,22 +477,22 @@ int norm_exponents(const double *X, long long sr, long long sk, int R, int K, in
                    void *scratch, cudaStream_t s) {
   const int chunks = K <= 1024 ? 1 : (K + 1023) / 1024 > 16 ? 16 : (K + 1023) / 1024;
   const int kchunk = (K + chunks - 1) / chunks;
-  int *pe = (int *)scratch;
-  int *pb = pe + (long long)chunks * R;
-  double *ps = (double *)round_up((uintptr_t)(pb + (long long)chunks * R), 16);
+  double *pmax = (double *)round_up((uintptr_t)scratch, 16);
+  double *pssq = pmax + (long long)chunks * R;
   if (sr == 1) {
     dim3 grid((R + 127) / 128, chunks);
     B2_PROF("ozaki_norm", s);
-    norm_partial_kernel<true><<<grid, 128, 0, s>>>(X, sr, sk, R, K, kchunk, pe, ps, pb);
+    norm_partial_kernel<true><<<grid, 128, 0, s>>>(X, sr, sk, R, K, kchunk, pmax, pssq);
   } else {
     dim3 grid((R + 7) / 8, chunks);
     B2_PROF("ozaki_norm", s);
-    norm_partial_kernel<false><<<grid, 256, 0, s>>>(X, sr, sk, R, K, kchunk, pe, ps, pb);
+    norm_partial_kernel<false><<<grid, 256, 0, s>>>(X, sr, sk, R, K, kchunk, pmax, pssq);
   }
   B2_CUDA_TRY(cudaGetLastError());
   {
     B2_PROF("ozaki_norm_finalize", s);
-    norm_finalize_kernel<<<(R + 255) / 256, 256, 0, s>>>(pe, ps, pb, R, chunks, H, sigma);
+    norm_finalize_kernel<<<(R + 255) / 256, 256, 0, s>>>(pmax, pssq, R, chunks, H, sigma, X, sr,
+                                                          sk, K);
   }
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
@@ -522,7 +591,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   }
   if (rc != B2_OK) return rc;
   {
-    const long long total = (long long)m * n;
+    const long long total = (long long)((m + 3) / 4) * n;
     const int blocks = (int)((total + 255) / 256 > 16384 ? 16384 : (total + 255) / 256);
     B2_PROF("ozaki_reconstruct", st);
     reconstruct_kernel<<<blocks, 256, 0, st>>>(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha,
@@ -686,7 +755,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
                                             derr, st, "ozaki_i8_gemm");
   if (rc != B2_OK) return rc;
   {
-    const long long total = (long long)m * n;
+    const long long total = (long long)((m + 3) / 4) * n;
     const int blocks = (int)((total + 255) / 256 > 16384 ? 16384 : (total + 255) / 256);
     reconstruct_kernel<<<blocks, 256, 0, st>>>(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha,
                                                 beta, C, ldc, A, asr, ask, B, bsk, bsr, k);
