@@ -36,6 +36,9 @@ int ozaki_auto_moduli(int k);
 int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                    const float *B, int ldb, float beta, float *C, int ldc, int method,
                    cudaStream_t s);
+int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                 const float *B, int ldb, float beta, float *C, int ldc, int method,
+                 cudaStream_t s);
 int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                const float *B, int ldb, float beta, float *C, int ldc, cudaStream_t s);
 

@@ -129,6 +129,10 @@ int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const flo
     case B2_METHOD_FP32:
     case B2_METHOD_DEFAULT:
       return sgemm_simt(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    case B2_METHOD_TF32:
+    case B2_METHOD_TF32X3:
+    case B2_METHOD_BF16X3:
+      return sgemm_tensor(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method, s);
     default:
       return B2_ERR_UNSUPPORTED;
   }

@@ -1,0 +1,171 @@
+// sgemm_tc.cu -- SGEMM on the tcgen05 tensor cores with FP32 accumulation.
+//
+// Replaces the reference's AVX-512 SGEMM (src/gemm_driver.c:116 built without
+// -DDOUBLE, OpenBLAS-like_implementation/sgemm.c:366-412) by three tensor-core
+// forms, all with FP32 accumulators in TMEM:
+//   TF32    1 product:  C = tf32(A) tf32(B)                     (kind::tf32)
+//   TF32X3  3 products: A = Ab + As, B = Bb + Bs (each TF32),
+//                       C = Ab Bb + Ab Bs + As Bb                (kind::tf32)
+//   BF16X3  3 products: A = Ah + Al, B = Bh + Bl (each BF16),
+//                       C = Ah Bh + Ah Bl + Al Bh                (kind::f16, bf16 in)
+// The split terms are laid side by side along K ([Bb|Bs|Bb] against
+// [Ab|Ab|As]), so every method is ONE GEMM over K' = terms * Kp on the
+// engine in umma.cuh; the split/convert kernel is the only extra pass.  Each
+// K segment is padded with zeros to a 128-byte K block.
+#include <cuda_bf16.h>
+
+#include "b2_methods.cuh"
+#include "b2_profile.cuh"
+#include "umma.cuh"
+
+namespace b2 {
+namespace {
+
+__device__ __forceinline__ float tf32_round(float x) {  // round to nearest, ties away
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// Writes `terms` K-segments per row of the operand viewed as R x K (element
+// (r,k) at X[r*sr + k*sk]) into out[r][terms*kp] (elements of type T).
+// pattern: which split part each segment holds (0 = big/high, 1 = small/low).
+template <typename T, bool ROWCONT>
+__global__ void __launch_bounds__(256)
+    split_kernel(const float *__restrict__ X, long long sr, long long sk, int R, int K, int kp,
+                 int terms, unsigned pattern, T *__restrict__ out) {
+  __shared__ float tile[32][65];
+  const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    const int idx = tid + 256 * e;
+    int rr, kk;
+    if (ROWCONT) { rr = idx & 31; kk = idx >> 5; } else { kk = idx & 63; rr = idx >> 6; }
+    const int r = r0 + rr, k = k0 + kk;
+    float v = 0.f;
+    if (r < R && k < K) v = __ldg(X + (long long)r * sr + (long long)k * sk);
+    tile[rr][kk] = v;
+  }
+  __syncthreads();
+  const int rr = tid >> 3, kg = (tid & 7) * 8;
+  const int r = r0 + rr;
+  if (r >= R || k0 + kg >= kp) return;  // pad columns [K, kp) are written as zeros below
+  T big[8], small[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float v = (k0 + kg + j < K) ? tile[rr][kg + j] : 0.f;
+    if constexpr (sizeof(T) == 4) {
+      const float b = tf32_round(v);
+      big[j] = b;
+      small[j] = tf32_round(v - b);
+    } else {
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      big[j] = h;
+      small[j] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+  }
+  T *row = out + (long long)r * terms * kp;
+  for (int t = 0; t < terms; ++t) {
+    const T *src = ((pattern >> t) & 1u) ? small : big;
+    T *dst = row + (long long)t * kp + k0 + kg;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dst[j] = src[j];
+  }
+}
+
+// FP32 epilogue: lane p = column n of C, columns q = rows m (contiguous in C).
+struct F32Epi {
+  float *C;
+  int ldc;
+  int M, N;
+  float alpha, beta;
+  __device__ __forceinline__ void operator()(int, int p, int q0, const uint32_t (&v)[32]) const {
+    if (p >= N || q0 >= M) return;
+    float *col = C + (long long)p * ldc + q0;
+    const int nq = min(32, M - q0);
+    const bool one = (beta == 1.f);
+    if (nq == 32 && ((((uintptr_t)col) & 15) == 0)) {
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        float4 c = reinterpret_cast<float4 *>(col)[g];
+        const float a0 = __uint_as_float(v[4 * g]), a1 = __uint_as_float(v[4 * g + 1]);
+        const float a2 = __uint_as_float(v[4 * g + 2]), a3 = __uint_as_float(v[4 * g + 3]);
+        c.x = one ? fmaf(alpha, a0, c.x) : fmaf(alpha, a0, beta * c.x);
+        c.y = one ? fmaf(alpha, a1, c.y) : fmaf(alpha, a1, beta * c.y);
+        c.z = one ? fmaf(alpha, a2, c.z) : fmaf(alpha, a2, beta * c.z);
+        c.w = one ? fmaf(alpha, a3, c.w) : fmaf(alpha, a3, beta * c.w);
+        reinterpret_cast<float4 *>(col)[g] = c;
+      }
+    } else {
+      for (int j = 0; j < nq; ++j) {
+        const float a = __uint_as_float(v[j]);
+        col[j] = one ? fmaf(alpha, a, col[j]) : fmaf(alpha, a, beta * col[j]);
+      }
+    }
+  }
+};
+
+inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+template <typename T>
+int run_split(const float *Xp, long long sr, long long sk, int R, int K, int kp, int terms,
+              unsigned pattern, T *out, cudaStream_t s) {
+  dim3 grid((kp + 63) / 64, (R + 31) / 32);
+  B2_PROF("sgemm_split", s);
+  if (sr == 1)
+    split_kernel<T, true><<<grid, 256, 0, s>>>(Xp, sr, sk, R, K, kp, terms, pattern, out);
+  else
+    split_kernel<T, false><<<grid, 256, 0, s>>>(Xp, sr, sk, R, K, kp, terms, pattern, out);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+}  // namespace
+
+int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                 const float *B, int ldb, float beta, float *C, int ldc, int method,
+                 cudaStream_t s) {
+  if (m <= 0 || n <= 0) return B2_OK;
+  Ctx *cx = ctx();
+  if (!cx) return B2_ERR_NO_DEVICE;
+  if (k <= 0 || alpha == 0.f) return beta == 1.f ? B2_OK : scale_matrix_s(m, n, beta, C, ldc, s);
+  const bool tA = !(ta == 'N' || ta == 'n');
+  const bool tB = !(tb == 'N' || tb == 'n');
+  const long long asr = tA ? lda : 1, ask = tA ? 1 : lda;   // op(A) rows m
+  const long long bsr = tB ? 1 : ldb, bsk = tB ? ldb : 1;   // op(B) columns n
+  const bool bf16 = (method == B2_METHOD_BF16X3);
+  const int terms = (method == B2_METHOD_TF32) ? 1 : 3;
+  const int esz = bf16 ? 2 : 4;
+  const int kp = (int)round_up(k, 128 / esz);
+  const long long kt = (long long)terms * kp;
+  void *Yp = workspace(cx, WS_SPLIT_Y, (size_t)m * kt * esz);
+  void *Xp = workspace(cx, WS_SPLIT_X, (size_t)n * kt * esz);
+  if (!Yp || !Xp) return B2_ERR_NOMEM;
+  // A side gets [big, big, small], B side [big, small, big]
+  const unsigned patA = 0x4u, patB = 0x2u;
+  int rc;
+  if (bf16) {
+    rc = run_split<__nv_bfloat16>(A, asr, ask, m, k, kp, terms, patA, (__nv_bfloat16 *)Yp, s);
+    if (rc == B2_OK)
+      rc = run_split<__nv_bfloat16>(B, bsr, bsk, n, k, kp, terms, patB, (__nv_bfloat16 *)Xp, s);
+  } else {
+    rc = run_split<float>(A, asr, ask, m, k, kp, terms, patA, (float *)Yp, s);
+    if (rc == B2_OK) rc = run_split<float>(B, bsr, bsk, n, k, kp, terms, patB, (float *)Xp, s);
+  }
+  if (rc != B2_OK) return rc;
+  const int kind = bf16 ? umma::KIND_BF16 : umma::KIND_TF32;
+  CUtensorMap tmX, tmY;
+  rc = umma::make_kmajor_map(&tmX, kind, Xp, kt, n, 1, kt * esz, (long long)n * kt * esz, umma::BM);
+  if (rc == B2_OK)
+    rc = umma::make_kmajor_map(&tmY, kind, Yp, kt, m, 1, kt * esz, (long long)m * kt * esz, 256);
+  if (rc != B2_OK) return rc;
+  F32Epi epi{C, ldc, m, n, alpha, beta};
+  if (bf16)
+    return umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
+                                                  cx->derr, s, "sgemm_umma_bf16");
+  return umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count, cx->derr,
+                                                s, "sgemm_umma_tf32");
+}
+
+}  // namespace b2
