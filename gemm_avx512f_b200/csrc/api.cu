@@ -225,6 +225,100 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
   return st;
 }
 
+static bool cnotrans(char c) { return c == 'N' || c == 'n' || c == 'R' || c == 'r'; }
+
+// Complex GEMM argument check: matrix rows follow the trans char ('N'/'R'
+// keep A as m x k, 'T'/'C'/other make it k x m).
+static int check_gemm3m(char ta, char tb, int m, int n, int k, int lda, int ldb, int ldc,
+                        const void *a, const void *b, const void *c, int *info) {
+  return check_gemm(cnotrans(ta) ? 'N' : 'T', cnotrans(tb) ? 'N' : 'T', m, n, k, lda, ldb, ldc,
+                    a, b, c, info);
+}
+
+template <typename T>
+static void gemm3m_dropin(const char *transa, const char *transb, const int *m, const int *n,
+                          const int *k, const T *alpha, const T *a, const int *lda, const T *b,
+                          const int *ldb, const T *beta, T *c, const int *ldc) {
+  if (!transa || !transb || !m || !n || !k || !alpha || !lda || !ldb || !beta || !ldc) {
+    set_status(B2_ERR_ARG, 0);
+    return;
+  }
+  const char ta = *transa, tb = *transb;
+  const int M = *m, N = *n, K = *k;
+  int info = 0;
+  int st = check_gemm3m(ta, tb, M, N, K, *lda, *ldb, *ldc, a, b, c, &info);
+  if (st != B2_OK) { set_status(st, info); return; }
+  if (M == 0 || N == 0) { set_status(B2_OK); return; }
+  Ctx *cx = ctx();
+  if (!cx) { set_status(B2_ERR_NO_DEVICE); return; }
+  cudaStream_t s = cx->stream;
+  const T al[2] = {alpha[0], alpha[1]}, be[2] = {beta[0], beta[1]};
+  const bool need_ab = K > 0 && !(al[0] == (T)0 && al[1] == (T)0);
+  const size_t esz = 2 * sizeof(T);
+  if (is_device_ptr(c) && (!need_ab || (is_device_ptr(a) && is_device_ptr(b)))) {
+    st = gemm3m_device<T>(ta, tb, M, N, K, al, a, *lda, b, *ldb, be, c, *ldc, s);
+  } else {
+    const int ra = cnotrans(ta) ? M : K, ca = cnotrans(ta) ? K : M;
+    const int rb = cnotrans(tb) ? K : N, cb = cnotrans(tb) ? N : K;
+    void *da = nullptr, *db = nullptr, *dc = nullptr;
+    int dla = 2, dlb = 2, dlc = 2;
+    st = B2_OK;
+    if (need_ab) {
+      st = stage_in(cx, WS_STAGE_A, a, ra, ca, *lda, esz, &da, &dla, s);
+      if (st == B2_OK) st = stage_in(cx, WS_STAGE_B, b, rb, cb, *ldb, esz, &db, &dlb, s);
+    }
+    if (st == B2_OK) st = stage_in(cx, WS_STAGE_C, c, M, N, *ldc, esz, &dc, &dlc, s);
+    if (st == B2_OK)
+      st = gemm3m_device<T>(ta, tb, M, N, K, al, (const T *)da, dla, (const T *)db, dlb, be,
+                            (T *)dc, dlc, s);
+    if (st == B2_OK) st = stage_out(c, *ldc, dc, dlc, M, N, esz, s);
+  }
+  if (st == B2_OK) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_fail(e, "stream sync");
+  }
+  set_status(st);
+}
+
+template <typename T>
+static int gemm3m_ext(char ta, char tb, int m, int n, int k, const T *alpha, const T *A, int lda,
+                      const T *B, int ldb, const T *beta, T *C, int ldc, void *stream) {
+  int info = 0;
+  if (!alpha || !beta) { set_status(B2_ERR_ARG, !alpha ? 6 : 11); return B2_ERR_ARG; }
+  int st = check_gemm3m(ta, tb, m, n, k, lda, ldb, ldc, A, B, C, &info);
+  if (st != B2_OK) { set_status(st, info); return st; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  const bool need_ab = k > 0 && !(alpha[0] == (T)0 && alpha[1] == (T)0);
+  if (m > 0 && n > 0 && (!is_device_ptr(C) || (need_ab && (!is_device_ptr(A) || !is_device_ptr(B))))) {
+    set_status(B2_ERR_ARG, !is_device_ptr(C) ? 12 : (!is_device_ptr(A) ? 7 : 9));
+    return B2_ERR_ARG;
+  }
+  st = gemm3m_device<T>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, pick_stream(c, stream));
+  set_status(st);
+  return st;
+}
+
+static bool lsame(char a, char b) { return a == b || a == b + 32; }
+
+// BLAS dtrsm argument check (xerbla positions).
+static int check_trsm(char side, char uplo, char transa, char diag, int m, int n, int lda,
+                      int ldb, const void *a, const void *b, int *info) {
+  const bool left = lsame(side, 'L');
+  const int nrowa = left ? m : n;
+  *info = 0;
+  if (!left && !lsame(side, 'R')) *info = 1;
+  else if (!lsame(uplo, 'U') && !lsame(uplo, 'L')) *info = 2;
+  else if (!lsame(transa, 'N') && !lsame(transa, 'T') && !lsame(transa, 'C')) *info = 3;
+  else if (!lsame(diag, 'U') && !lsame(diag, 'N')) *info = 4;
+  else if (m < 0) *info = 5;
+  else if (n < 0) *info = 6;
+  else if (lda < (nrowa > 1 ? nrowa : 1)) *info = 9;
+  else if (ldb < (m > 1 ? m : 1)) *info = 11;
+  else if (m > 0 && n > 0 && (!a || !b)) *info = !a ? 8 : 10;
+  return *info ? B2_ERR_ARG : B2_OK;
+}
+
 }  // namespace b2
 
 using namespace b2;
@@ -318,6 +412,91 @@ void SGEMM_(const char *transa, const char *transb, const int *m, const int *n, 
             const float *alpha, const float *a, const int *lda, const float *b, const int *ldb,
             const float *beta, float *c, const int *ldc) {
   sgemm_(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+void zgemm3m_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+              const double *alpha, const double *a, const int *lda, const double *b,
+              const int *ldb, const double *beta, double *c, const int *ldc) {
+  gemm3m_dropin<double>(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+void cgemm3m_(const char *transa, const char *transb, const int *m, const int *n, const int *k,
+              const float *alpha, const float *a, const int *lda, const float *b,
+              const int *ldb, const float *beta, float *c, const int *ldc) {
+  gemm3m_dropin<float>(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc);
+}
+
+int b2_zgemm3m(char transa, char transb, int m, int n, int k, const double *alpha,
+               const double *A, int lda, const double *B, int ldb, const double *beta, double *C,
+               int ldc, void *stream) {
+  return gemm3m_ext<double>(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
+}
+
+int b2_cgemm3m(char transa, char transb, int m, int n, int k, const float *alpha,
+               const float *A, int lda, const float *B, int ldb, const float *beta, float *C,
+               int ldc, void *stream) {
+  return gemm3m_ext<float>(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, stream);
+}
+
+void dtrsm_(const char *side, const char *uplo, const char *transa, const char *diag,
+            const int *m, const int *n, const double *alpha, const double *a, const int *lda,
+            double *b, const int *ldb) {
+  if (!side || !uplo || !transa || !diag || !m || !n || !alpha || !lda || !ldb) {
+    set_status(B2_ERR_ARG, 0);
+    return;
+  }
+  const int M = *m, N = *n;
+  int info = 0;
+  int st = check_trsm(*side, *uplo, *transa, *diag, M, N, *lda, *ldb, a, b, &info);
+  if (st != B2_OK) { set_status(st, info); return; }
+  if (M == 0 || N == 0) { set_status(B2_OK); return; }
+  Ctx *cx = ctx();
+  if (!cx) { set_status(B2_ERR_NO_DEVICE); return; }
+  cudaStream_t s = cx->stream;
+  const int na = lsame(*side, 'L') ? M : N;
+  if (is_device_ptr(b) && is_device_ptr(a)) {
+    st = dtrsm_device(*side, *uplo, *transa, *diag, M, N, *alpha, a, *lda, b, *ldb,
+                      cx->dgemm_method, 0, s);
+  } else {
+    void *da = nullptr, *db = nullptr;
+    int dla = 2, dlb = 2;
+    st = stage_in(cx, WS_TRSM, a, na, na, *lda, sizeof(double), &da, &dla, s);
+    if (st == B2_OK) st = stage_in(cx, WS_STAGE_C, b, M, N, *ldb, sizeof(double), &db, &dlb, s);
+    if (st == B2_OK)
+      st = dtrsm_device(*side, *uplo, *transa, *diag, M, N, *alpha, (const double *)da, dla,
+                        (double *)db, dlb, cx->dgemm_method, 0, s);
+    if (st == B2_OK) st = stage_out(b, *ldb, db, dlb, M, N, sizeof(double), s);
+  }
+  if (st == B2_OK) {
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = cuda_fail(e, "stream sync");
+  }
+  set_status(st);
+}
+
+int b2_dtrsm(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+             const double *A, int lda, double *B, int ldb, int update_method, int block,
+             void *stream) {
+  int info = 0;
+  int st = check_trsm(side, uplo, transa, diag, m, n, lda, ldb, A, B, &info);
+  if (st != B2_OK) { set_status(st, info); return st; }
+  if (m == 0 || n == 0) { set_status(B2_OK); return B2_OK; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  if (!is_device_ptr(B) || !is_device_ptr(A)) {
+    set_status(B2_ERR_ARG, !is_device_ptr(A) ? 8 : 10);
+    return B2_ERR_ARG;
+  }
+  if (!(update_method == B2_METHOD_DEFAULT || update_method == B2_METHOD_FP64 ||
+        update_method == B2_METHOD_OZAKI || update_method == B2_METHOD_AUTO) ||
+      block < 0 || block > 128) {
+    set_status(B2_ERR_ARG, 12);
+    return B2_ERR_ARG;
+  }
+  st = dtrsm_device(side, uplo, transa, diag, m, n, alpha, A, lda, B, ldb, update_method, block,
+                    pick_stream(c, stream));
+  set_status(st);
+  return st;
 }
 
 int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha, const double *A,

@@ -31,7 +31,7 @@ enum WsSlot {
   WS_STAGE_A = 0, WS_STAGE_B, WS_STAGE_C,   // host-pointer staging
   WS_OZ_X, WS_OZ_Y, WS_OZ_R, WS_OZ_SCALE,   // Ozaki slices / residues / exponents
   WS_SPLIT_X, WS_SPLIT_Y,                   // SGEMM split planes
-  WS_TRSM, WS_3M, WS_GROUP, WS_ERR, WS_MISC,
+  WS_TRSM, WS_TRSM_INV, WS_TRSM_TMP, WS_3M, WS_GROUP, WS_ERR, WS_MISC,
   WS_COUNT
 };
 

@@ -42,4 +42,14 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
 int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                const float *B, int ldb, float beta, float *C, int ldc, cudaStream_t s);
 
+// Blocked triangular solve (trsm.cu).
+int dtrsm_device(char side, char uplo, char transa, char diag, int m, int n, double alpha,
+                 const double *A, int lda, double *B, int ldb, int method, int block,
+                 cudaStream_t s);
+
+// 3M complex GEMM, one fused launch (gemm3m.cu); alpha/beta are (re, im) pairs.
+template <typename T>
+int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T *A, int lda,
+                  const T *B, int ldb, const T *beta, T *C, int ldc, cudaStream_t s);
+
 }  // namespace b2

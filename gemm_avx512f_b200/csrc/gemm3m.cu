@@ -1,0 +1,288 @@
+// gemm3m.cu -- complex GEMM by the 3M method in ONE fused launch.
+//
+// Replaces the OpenBLAS gemm3m driver + the reference's 3M kernels
+// (zgemm3m_kernel_2x8_skylakex.c:336-351, zgemm3m_kernel_8x4_skylakex.c:309-334,
+// cgemm3m_kernel_16x4_skylakex.c:415-440).  The reference kernels compute
+// C_cplx += (alpha_r + i alpha_i) (A_real_packed . B_real_packed) and are called
+// three times by the driver on pre-added panels.  Here every CTA owns one tile
+// of C and forms all three real products from the same staged tiles:
+//     P1 = Ar Br,  P2 = Ai Bi,  P3 = (Ar + Ai)(Br + Bi)
+//     Re(AB) = P1 - P2,  Im(AB) = P3 - P1 - P2
+// The pre-additions (and conjugation for 'C'/'R') happen while the complex
+// tiles are de-interleaved into shared memory; the post-additions and the
+// complex alpha/beta happen in the epilogue.  beta follows the reference
+// drivers (C scaled whenever beta != 1, src/gemm_driver.c:131).
+//   zgemm3m: FP64 DMMA (mma.sync.m16n8k4.f64), 64x64 tile, 8 warps of 32x16.
+//   cgemm3m: FP32 FFMA, 64x64 tile, 256 threads of 4x4 outputs.
+#include "b2_methods.cuh"
+#include "b2_profile.cuh"
+
+namespace b2 {
+namespace {
+
+constexpr int G_BM = 64, G_BN = 64, G_BK = 16, G_PAD = 4;
+constexpr int G_LD = G_BM + G_PAD;  // [k][m] / [k][n] row stride (68 = 4 mod 16 doubles)
+
+__device__ __forceinline__ bool tr_is_t(char c) {
+  return !(c == 'N' || c == 'n' || c == 'R' || c == 'r');
+}
+__device__ __forceinline__ bool tr_is_conj(char c) {
+  return c == 'C' || c == 'c' || c == 'R' || c == 'r';
+}
+
+// Stage one BK-deep complex K panel of op(A) (G_BM rows) and op(B) (G_BN
+// columns) into registers.  Element (m,k) of op(A) is A[m*lda+k] when
+// transposed, else A[k*lda+m] (complex units); element (k,n) of op(B) is
+// B[k*ldb+n] when transposed, else B[n*ldb+k].
+template <typename T, int NT>
+struct Stage3M {
+  static constexpr int PER = G_BM * G_BK / NT;  // complex elements per thread per operand
+  T ar[PER], ai[PER], br[PER], bi[PER];
+  __device__ __forceinline__ void load(const T *A, int lda, const T *B, int ldb, int M, int N,
+                                       int K, int m0, int n0, int k0, bool tA, bool tB,
+                                       T sa, T sb, int tid) {
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const int idx = tid + NT * e;
+      int mm, kk;
+      if (tA) { kk = idx % G_BK; mm = idx / G_BK; } else { mm = idx % G_BM; kk = idx / G_BM; }
+      const int gm = m0 + mm, gk = k0 + kk;
+      T re = 0, im = 0;
+      if (gm < M && gk < K) {
+        const T *p = A + 2 * (tA ? ((long long)gm * lda + gk) : ((long long)gk * lda + gm));
+        re = p[0];
+        im = sa * p[1];
+      }
+      ar[e] = re;
+      ai[e] = im;
+      int nn;
+      if (tB) { nn = idx % G_BN; kk = idx / G_BN; } else { kk = idx % G_BK; nn = idx / G_BK; }
+      const int gn = n0 + nn, gk2 = k0 + kk;
+      re = 0;
+      im = 0;
+      if (gn < N && gk2 < K) {
+        const T *p = B + 2 * (tB ? ((long long)gk2 * ldb + gn) : ((long long)gn * ldb + gk2));
+        re = p[0];
+        im = sb * p[1];
+      }
+      br[e] = re;
+      bi[e] = im;
+    }
+  }
+  // shared layout: [3][BK][G_LD] for A (r, i, r+i) and the same for B
+  __device__ __forceinline__ void store(T *sA, T *sB, bool tA, bool tB, int tid) const {
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+      const int idx = tid + NT * e;
+      int mm, kk;
+      if (tA) { kk = idx % G_BK; mm = idx / G_BK; } else { mm = idx % G_BM; kk = idx / G_BM; }
+      sA[(0 * G_BK + kk) * G_LD + mm] = ar[e];
+      sA[(1 * G_BK + kk) * G_LD + mm] = ai[e];
+      sA[(2 * G_BK + kk) * G_LD + mm] = ar[e] + ai[e];
+      int nn;
+      if (tB) { nn = idx % G_BN; kk = idx / G_BN; } else { kk = idx % G_BK; nn = idx / G_BK; }
+      sB[(0 * G_BK + kk) * G_LD + nn] = br[e];
+      sB[(1 * G_BK + kk) * G_LD + nn] = bi[e];
+      sB[(2 * G_BK + kk) * G_LD + nn] = br[e] + bi[e];
+    }
+  }
+};
+
+template <typename T>
+__device__ __forceinline__ void epilogue3m(T *C, int ldc, int m, int n, T p1, T p2, T p3,
+                                           T ar, T ai, T br, T bi) {
+  const T re = p1 - p2, im = p3 - p1 - p2;
+  T *c = C + 2 * ((long long)n * ldc + m);
+  T cr = c[0], ci = c[1];
+  if (!(br == (T)1 && bi == (T)0)) {
+    const T tr = br * cr - bi * ci, ti = br * ci + bi * cr;
+    cr = tr;
+    ci = ti;
+  }
+  c[0] = cr + (ar * re - ai * im);
+  c[1] = ci + (ar * im + ai * re);
+}
+
+// ---------------------------------------------------- zgemm3m: FP64 DMMA --
+__global__ void __launch_bounds__(256)
+    zgemm3m_kernel(int M, int N, int K, const double *__restrict__ A, int lda,
+                   const double *__restrict__ B, int ldb, double *__restrict__ C, int ldc,
+                   double ar, double ai, double br, double bi, char transa, char transb) {
+  extern __shared__ __align__(16) double zsm[];  // [2][3*BK*LD] A, then [2][3*BK*LD] B
+  double *sA[2] = {zsm, zsm + 3 * G_BK * G_LD};
+  double *sB[2] = {zsm + 6 * G_BK * G_LD, zsm + 9 * G_BK * G_LD};
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp >> 2) * 32, wn0 = (warp & 3) * 16;
+  const int m0 = blockIdx.x * G_BM, n0 = blockIdx.y * G_BN;
+  const bool tA = tr_is_t(transa), tB = tr_is_t(transb);
+  const double sa = tr_is_conj(transa) ? -1.0 : 1.0, sb = tr_is_conj(transb) ? -1.0 : 1.0;
+  double acc[3][2][2][4];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[p][i][j][v] = 0.0;
+
+  Stage3M<double, 256> st;
+  const int KT = (K + G_BK - 1) / G_BK;
+  st.load(A, lda, B, ldb, M, N, K, m0, n0, 0, tA, tB, sa, sb, tid);
+  st.store(sA[0], sB[0], tA, tB, tid);
+  __syncthreads();
+  for (int kt = 0; kt < KT; ++kt) {
+    const int buf = kt & 1;
+    if (kt + 1 < KT) st.load(A, lda, B, ldb, M, N, K, m0, n0, (kt + 1) * G_BK, tA, tB, sa, sb, tid);
+    const double *As = sA[buf], *Bs = sB[buf];
+#pragma unroll
+    for (int kk = 0; kk < G_BK; kk += 4) {
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        double af[2][2], bf[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int v = 0; v < 2; ++v)
+            af[i][v] = As[(p * G_BK + kk + t) * G_LD + wm0 + i * 16 + g + 8 * v];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) bf[j] = Bs[(p * G_BK + kk + t) * G_LD + wn0 + j * 8 + g];
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            asm volatile(
+                "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, "
+                "{%6}, {%0,%1,%2,%3};\n"
+                : "+d"(acc[p][i][j][0]), "+d"(acc[p][i][j][1]), "+d"(acc[p][i][j][2]),
+                  "+d"(acc[p][i][j][3])
+                : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
+      }
+    }
+    if (kt + 1 < KT) {
+      st.store(sA[buf ^ 1], sB[buf ^ 1], tA, tB, tid);
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int m = m0 + wm0 + i * 16 + g + 8 * (v >> 1);
+        const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
+        if (m < M && n < N)
+          epilogue3m<double>(C, ldc, m, n, acc[0][i][j][v], acc[1][i][j][v], acc[2][i][j][v],
+                             ar, ai, br, bi);
+      }
+}
+
+// ---------------------------------------------------- cgemm3m: FP32 FFMA --
+__global__ void __launch_bounds__(256)
+    cgemm3m_kernel(int M, int N, int K, const float *__restrict__ A, int lda,
+                   const float *__restrict__ B, int ldb, float *__restrict__ C, int ldc,
+                   float ar, float ai, float br, float bi, char transa, char transb) {
+  extern __shared__ __align__(16) float csm[];
+  float *sA[2] = {csm, csm + 3 * G_BK * G_LD};
+  float *sB[2] = {csm + 6 * G_BK * G_LD, csm + 9 * G_BK * G_LD};
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * G_BM, n0 = blockIdx.y * G_BN;
+  const bool tA = tr_is_t(transa), tB = tr_is_t(transb);
+  const float sa = tr_is_conj(transa) ? -1.f : 1.f, sb = tr_is_conj(transb) ? -1.f : 1.f;
+  float acc[3][4][4];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[p][i][j] = 0.f;
+  Stage3M<float, 256> st;
+  const int KT = (K + G_BK - 1) / G_BK;
+  st.load(A, lda, B, ldb, M, N, K, m0, n0, 0, tA, tB, sa, sb, tid);
+  st.store(sA[0], sB[0], tA, tB, tid);
+  __syncthreads();
+  for (int kt = 0; kt < KT; ++kt) {
+    const int buf = kt & 1;
+    if (kt + 1 < KT) st.load(A, lda, B, ldb, M, N, K, m0, n0, (kt + 1) * G_BK, tA, tB, sa, sb, tid);
+    const float *As = sA[buf], *Bs = sB[buf];
+#pragma unroll
+    for (int kk = 0; kk < G_BK; ++kk) {
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        const float4 a = *reinterpret_cast<const float4 *>(&As[(p * G_BK + kk) * G_LD + tx * 4]);
+        const float4 b = *reinterpret_cast<const float4 *>(&Bs[(p * G_BK + kk) * G_LD + ty * 4]);
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[p][i][j] = fmaf(av[i], bv[j], acc[p][i][j]);
+      }
+    }
+    if (kt + 1 < KT) {
+      st.store(sA[buf ^ 1], sB[buf ^ 1], tA, tB, tid);
+      __syncthreads();
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int m = m0 + tx * 4 + i, n = n0 + ty * 4 + j;
+      if (m < M && n < N)
+        epilogue3m<float>(C, ldc, m, n, acc[0][i][j], acc[1][i][j], acc[2][i][j], ar, ai, br, bi);
+    }
+}
+
+template <typename T>
+__global__ void cscale_kernel(int M, int N, T br, T bi, T *__restrict__ C, int ldc) {
+  const long long total = (long long)M * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int m = (int)(idx % M), n = (int)(idx / M);
+    T *c = C + 2 * ((long long)n * ldc + m);
+    const T cr = c[0], ci = c[1];
+    c[0] = br * cr - bi * ci;
+    c[1] = br * ci + bi * cr;
+  }
+}
+
+}  // namespace
+
+template <typename T>
+int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T *A, int lda,
+                  const T *B, int ldb, const T *beta, T *C, int ldc, cudaStream_t s) {
+  if (m <= 0 || n <= 0) return B2_OK;
+  const T ar = alpha[0], ai = alpha[1], br = beta[0], bi = beta[1];
+  if (k <= 0 || (ar == (T)0 && ai == (T)0)) {
+    if (br == (T)1 && bi == (T)0) return B2_OK;
+    const long long total = (long long)m * n;
+    const int blocks = (int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256);
+    B2_PROF("gemm3m_scale", s);
+    cscale_kernel<T><<<blocks, 256, 0, s>>>(m, n, br, bi, C, ldc);
+    B2_CUDA_TRY(cudaGetLastError());
+    return B2_OK;
+  }
+  dim3 grid((m + G_BM - 1) / G_BM, (n + G_BN - 1) / G_BN);
+  const int smem = (int)(12 * G_BK * G_LD * sizeof(T));
+  if constexpr (sizeof(T) == 8) {
+    B2_CUDA_TRY(cudaFuncSetAttribute(zgemm3m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2_PROF("zgemm3m_fused", s);
+    zgemm3m_kernel<<<grid, 256, smem, s>>>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, ta, tb);
+  } else {
+    B2_CUDA_TRY(cudaFuncSetAttribute(cgemm3m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    B2_PROF("cgemm3m_fused", s);
+    cgemm3m_kernel<<<grid, 256, smem, s>>>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, ta, tb);
+  }
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+template int gemm3m_device<double>(char, char, int, int, int, const double *, const double *, int,
+                                   const double *, int, const double *, double *, int,
+                                   cudaStream_t);
+template int gemm3m_device<float>(char, char, int, int, int, const float *, const float *, int,
+                                  const float *, int, const float *, float *, int, cudaStream_t);
+
+}  // namespace b2

@@ -473,9 +473,21 @@ int upload_table(int s, int dev, cudaStream_t st) {
 inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
 
 // Exponents for the R "rows" of an operand (element (r,k) at X[r*sr + k*sk]).
+// K chunks of the norm pass: about one per 1024 of K, more when there are few
+// rows (so at least ~16k rows x chunks are in flight), never below 64 of K each.
+int norm_chunks(int R, int K) {
+  int c = (K + 1023) / 1024;
+  if (c > 16) c = 16;
+  const int want = (16384 + R - 1) / (R > 0 ? R : 1);
+  if (c < want) c = want;
+  if (c > 64) c = 64;
+  const int maxc = K / 64 > 1 ? K / 64 : 1;
+  return c < maxc ? c : maxc;
+}
+
 int norm_exponents(const double *X, long long sr, long long sk, int R, int K, int H, int *sigma,
                    void *scratch, cudaStream_t s) {
-  const int chunks = K <= 1024 ? 1 : (K + 1023) / 1024 > 16 ? 16 : (K + 1023) / 1024;
+  const int chunks = norm_chunks(R, K);
   const int kchunk = (K + chunks - 1) / chunks;
   double *pmax = (double *)round_up((uintptr_t)scratch, 16);
   double *pssq = pmax + (long long)chunks * R;
@@ -499,7 +511,7 @@ int norm_exponents(const double *X, long long sr, long long sk, int R, int K, in
 }
 
 size_t norm_scratch_bytes(int R, int K) {
-  const int chunks = K <= 1024 ? 1 : (K + 1023) / 1024 > 16 ? 16 : (K + 1023) / 1024;
+  const int chunks = norm_chunks(R, K);
   return (size_t)chunks * R * 16 + 64;
 }
 
@@ -629,7 +641,7 @@ extern "C" int b2_ozaki_last_plan(int *out, int n) {
 // Limits and sharing: a call needs
 //   s*(m*kp + n*kp + n*mp) + (m + n)*(4 + 16*chunks) bytes (+ alignment),
 // kp = K rounded up to 16 (K <= 65536), mp = m rounded up to 16, s = moduli,
-// chunks = min(16, ceil(K/1024)); anything above B2_NOALLOC_SCRATCH_BYTES is
+// chunks = norm pass K chunks (<= 64); anything above B2_NOALLOC_SCRATCH_BYTES is
 // rejected with B2_ERR_ARG.  All calls on a device share the one array and
 // it keeps the previous call's contents, so calls that overlap on the GPU
 // (different streams, or different host threads) race; serialise them.

@@ -248,10 +248,14 @@ static int is_unit(char c) { return c == 'U' || c == 'u'; }
 void oracle_dtrsm(char side, char uplo, char transa, char diag, int M, int N, double alpha,
                   const double *A, int lda, double *B, int ldb, int nb) {
   if (M <= 0 || N <= 0) return;
+  if (alpha == 0.0) { /* BLAS: B := 0 */
+    for (int j = 0; j < N; j++)
+      for (int i = 0; i < M; i++) B[(int64_t)j * ldb + i] = 0.0;
+    return;
+  }
   if (alpha != 1.0)
     for (int j = 0; j < N; j++)
       for (int i = 0; i < M; i++) B[(int64_t)j * ldb + i] *= alpha;
-  if (alpha == 0.0) return;
   const int left = is_left(side), up = is_upper(uplo), nt = notrans(transa), unit = is_unit(diag);
 #define AEL(i, j) A[(int64_t)(j) * lda + (i)]
 #define BEL(i, j) B[(int64_t)(j) * ldb + (i)]

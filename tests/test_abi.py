@@ -75,3 +75,19 @@ def test_status_strings():
     L = _lib.lib()
     for s in range(7):
         assert L.b2_status_string(s)
+
+
+@pytest.mark.parametrize("args,info", [
+    (dict(side="X"), 1), (dict(uplo="Q"), 2), (dict(transa="Z"), 3), (dict(diag="W"), 4),
+    (dict(m=-1), 5), (dict(n=-1), 6), (dict(lda=3), 9), (dict(ldb=2), 11)])
+def test_dtrsm_argument_errors_leave_b_untouched(args, info):
+    a = np.eye(8, order="F")
+    b = np.full((8, 8), 5.0, order="F")
+    before = b.copy()
+    kw = dict(side="L", uplo="L", transa="N", diag="N", m=6, n=5, lda=8, ldb=8)
+    kw.update(args)
+    with pytest.raises(_lib.B2Error) as ei:
+        blas.dtrsm(kw["side"], kw["uplo"], kw["transa"], kw["diag"], kw["m"], kw["n"], 1.0, a,
+                   kw["lda"], b, kw["ldb"])
+    assert ei.value.status == _lib.B2_ERR_ARG and ei.value.info == info
+    assert np.array_equal(b, before)

@@ -1,0 +1,95 @@
+"""GPU tests of the fused 3M complex GEMMs (zgemm3m_ on FP64 DMMA, cgemm3m_ on
+FP32 FFMA), through the C ABI.
+
+* parity with the CPU 3M restatement (oracle_zgemm3m / oracle_cgemm3m, whose
+  real products run through the bit-exact restatement of the reference dgemm_):
+  ||C - C_ref||_F / (K u ||A||_F ||B||_F) <= 8 on complex Frobenius norms;
+* pinned to the reference's own zgemm3m kernel (zgemm3m_kernel_2x8_skylakex.c:
+  C_cplx += alpha * A_real B_real^T) through the golden vectors: real
+  operands passed as complex with zero imaginary part and beta = 1;
+* all four op() forms ('N', 'T', 'C' conjugate-transpose, 'R' conjugate),
+  padded leading dimensions left untouched, reference beta semantics.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from gemm_avx512f_b200 import blas
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _op(x, t):
+    return {"N": x, "T": x.T, "C": x.conj().T, "R": x.conj()}[t]
+
+
+def _cmat(rng, r, c, dtype, pad=0):
+    x = rng.uniform(-1, 1, (r + pad, c)) + 1j * rng.uniform(-1, 1, (r + pad, c))
+    return np.asfortranarray(x.astype(dtype))
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (13, 9, 21), (65, 33, 129), (200, 150, 300),
+                                   (512, 512, 512)])
+def test_gemm3m_parity(cuda, dtype, m, n, k):
+    rng = np.random.default_rng(m + 2 * n + 3 * k)
+    u = np.finfo(dtype).eps / 2
+    fn = blas.zgemm3m if dtype == np.complex128 else blas.cgemm3m
+    for ta, tb in [("N", "N"), ("T", "C"), ("C", "N"), ("R", "T")]:
+        ar, ac = (m, k) if ta in "NR" else (k, m)
+        br, bc = (k, n) if tb in "NR" else (n, k)
+        a = _cmat(rng, ar, ac, dtype, pad=2)
+        b = _cmat(rng, br, bc, dtype, pad=1)
+        c = _cmat(rng, m, n, dtype, pad=3)
+        al, be = 0.75 - 1.25j, 0.5 + 0.25j
+        ref = c.copy(order="F")
+        O.gemm3m(ta, tb, m, n, k, al, a[:ar], b[:br], be, ref[:m])
+        got = c.copy(order="F")
+        fn(ta, tb, m, n, k, al, a, a.shape[0], b, b.shape[0], be, got, got.shape[0])
+        assert np.array_equal(got[m:], c[m:]), "padding rows of C were written"
+        den = k * u * np.linalg.norm(a[:ar]) * np.linalg.norm(b[:br])
+        err = np.linalg.norm((got[:m] - ref[:m]).astype(np.complex128)) / den
+        assert err <= 8, (dtype, m, n, k, ta, tb, err)
+        # and it is the complex product
+        exact = al * _op(a[:ar].astype(np.complex128), ta) @ _op(b[:br].astype(np.complex128), tb) \
+            + be * c[:m].astype(np.complex128)
+        assert np.linalg.norm(got[:m] - exact) <= 64 * den
+
+
+def test_pinned_to_reference_3m_kernel_golden(cuda):
+    z = np.load(os.path.join(GOLD, "zgemm3m_kernel_ref.npz"))
+    for i in range(int(z["count"])):
+        m, n, k = (int(v) for v in z[f"z{i}_meta"])
+        ar, ai = (float(v) for v in z[f"z{i}_alpha"])
+        a = np.asfortranarray(z[f"z{i}_a"].astype(np.complex128))   # m x k, imag 0
+        b = np.asfortranarray(z[f"z{i}_b"].astype(np.complex128))   # n x k, imag 0
+        c = np.asfortranarray(z[f"z{i}_c"].copy())                 # (m+1) x n
+        blas.zgemm3m("N", "T", m, n, k, complex(ar, ai), a, m, b, n, 1.0, c, c.shape[0])
+        np.testing.assert_allclose(c, z[f"z{i}_out"], rtol=0, atol=1e-13)
+
+
+def test_gemm3m_beta_semantics_and_device_api(cuda):
+    import torch
+
+    m, n, k = 40, 30, 20
+    rng = np.random.default_rng(0)
+    a = _cmat(rng, m, k, np.complex128)
+    b = _cmat(rng, k, n, np.complex128)
+    c = np.asfortranarray(np.full((m, n), np.nan + 0j))
+    blas.zgemm3m("N", "N", m, n, k, 1.0, a, m, b, k, 0.0, c, m)
+    assert np.isnan(c.real).all()  # beta == 0 keeps NaN (reference beta rule)
+    # alpha == 0 skips the product: C <- beta C exactly
+    c2 = _cmat(rng, m, n, np.complex128)
+    got = c2.copy(order="F")
+    blas.zgemm3m("N", "N", m, n, k, 0.0, a, m, b, k, 2.0, got, m)
+    assert np.array_equal(got, 2.0 * c2)
+    # device pointers through b2_zgemm3m
+    da = torch.from_numpy(np.ascontiguousarray(a.T)).to(cuda)  # column-major complex
+    db = torch.from_numpy(np.ascontiguousarray(b.T)).to(cuda)
+    dc = torch.zeros((n, m), dtype=torch.complex128, device=cuda)
+    blas.zgemm3m_device("N", "N", m, n, k, 1.0, da, m, db, k, 0.0, dc, m)
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(dc.cpu().numpy().T, a @ b, rtol=0, atol=1e-12)

@@ -162,3 +162,33 @@ def test_comparer_flags_planted_corruption():
     u = np.finfo(np.float32).eps / 2
     assert normalized(good, ref, k, a, b, u) <= 8
     assert normalized(bad, ref, k, a, b, u) > 8
+
+
+def test_blas_trsm_oracle_agrees_with_reference_lt_kernel_semantics():
+    """The tester's 'lt' reference (dtrsm_kernel_16x4_tester.c:160-199) solves a
+    lower triangle packed with its diagonal inverted, after adding the GEMM
+    update sb to C.  Unpacking that triangle and calling the BLAS-level
+    oracle_dtrsm (Left/Lower/NoTrans) on C + update gives the same X."""
+    rng = np.random.default_rng(11)
+    M, N = 16, 12
+    sa = rng.uniform(0.5, 1.5, M * M)
+    # lower triangle L with L[i, i] = 1 / sa[i*M + i] and L[i, k] = sa[k*M + i] for i > k
+    L = np.zeros((M, M))
+    for k in range(M):
+        L[k, k] = 1.0 / sa[k * M + k]
+        for i in range(k + 1, M):
+            L[i, k] = sa[k * M + i]
+    sb = rng.uniform(-1, 1, N * M)
+    C = rng.uniform(-1, 1, M * N)
+    c_kern = C.copy()
+    O.trsm_kernel("lt", M, N, sa.copy(), sb.copy(), c_kern, M, M)
+    upd = np.zeros((M, N))
+    n0 = 0
+    while n0 < N:  # sb holds the update in 4-column panels, k-major within a panel
+        w = min(4, N - n0)
+        blk = sb[n0 * M: n0 * M + w * M].reshape(M, w)
+        upd[:, n0:n0 + w] = blk
+        n0 += w
+    rhs = np.asfortranarray(C.reshape(N, M).T + upd)
+    x = O.trsm("L", "L", "N", "N", M, N, 1.0, np.asfortranarray(L), rhs, nb=0)
+    np.testing.assert_allclose(x, c_kern.reshape(N, M).T, rtol=0, atol=1e-12)
