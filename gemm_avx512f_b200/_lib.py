@@ -30,6 +30,15 @@ METHODS = {
 _lib: C.CDLL | None = None
 
 
+class GemmProblem(C.Structure):
+    """Mirror of b2_gemm_problem (include/b2blas.h)."""
+    _fields_ = [("dtype", C.c_int), ("transa", C.c_char), ("transb", C.c_char),
+                ("m", C.c_int), ("n", C.c_int), ("k", C.c_int),
+                ("alpha", C.c_double), ("beta", C.c_double),
+                ("A", C.c_void_p), ("lda", C.c_int), ("B", C.c_void_p), ("ldb", C.c_int),
+                ("C", C.c_void_p), ("ldc", C.c_int)]
+
+
 class B2Error(RuntimeError):
     def __init__(self, status: int, info: int = 0, what: str = ""):
         self.status, self.info = status, info
@@ -84,6 +93,13 @@ def lib() -> C.CDLL:
     L.b2_device_error.argtypes = [i]
     L.b2_dgemm_ozaki_noalloc.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, p]
     L.b2_dgemm_ozaki_noalloc.restype = i
+    L.b2_gemm_grouped.argtypes = [i, p, p]
+    L.b2_grouped_plan_create.argtypes = [i, p, C.POINTER(C.c_void_p)]
+    L.b2_grouped_plan_launch.argtypes = [p, p]
+    L.b2_grouped_plan_destroy.argtypes = [p]
+    for nm in ("b2_gemm_grouped", "b2_grouped_plan_create", "b2_grouped_plan_launch",
+               "b2_grouped_plan_destroy"):
+        getattr(L, nm).restype = i
     L.b2_set_fp64_config.argtypes = [i, i, i]
     L.b2_set_fp64_config.restype = i
     L.b2_launch_count.restype = C.c_longlong

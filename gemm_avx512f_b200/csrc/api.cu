@@ -499,6 +499,38 @@ int b2_dtrsm(char side, char uplo, char transa, char diag, int m, int n, double 
   return st;
 }
 
+int b2_gemm_grouped(int count, const b2_gemm_problem *problems, void *stream) {
+  if (count < 0 || (count > 0 && !problems)) { set_status(B2_ERR_ARG, 0); return B2_ERR_ARG; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  int info = 0;
+  const int st = grouped_device(count, problems, pick_stream(c, stream), &info);
+  set_status(st, info);
+  return st;
+}
+
+int b2_grouped_plan_create(int count, const b2_gemm_problem *problems, void **plan) {
+  if (count < 0 || (count > 0 && !problems) || !plan) { set_status(B2_ERR_ARG, 0); return B2_ERR_ARG; }
+  int info = 0;
+  const int st = grouped_plan_create(count, problems, plan, &info);
+  set_status(st, info);
+  return st;
+}
+
+int b2_grouped_plan_launch(void *plan, void *stream) {
+  if (!plan) { set_status(B2_ERR_ARG, 1); return B2_ERR_ARG; }
+  Ctx *c = ctx();
+  if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+  const int st = grouped_plan_launch(plan, pick_stream(c, stream));
+  set_status(st);
+  return st;
+}
+
+int b2_grouped_plan_destroy(void *plan) {
+  if (!plan) return B2_OK;
+  return grouped_plan_destroy(plan);
+}
+
 int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha, const double *A,
              int lda, const double *B, int ldb, double beta, double *C, int ldc, int method,
              int slices, void *stream) {

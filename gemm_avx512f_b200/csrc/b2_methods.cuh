@@ -47,6 +47,12 @@ int dtrsm_device(char side, char uplo, char transa, char diag, int m, int n, dou
                  const double *A, int lda, double *B, int ldb, int method, int block,
                  cudaStream_t s);
 
+// Grouped GEMM (grouped.cu).
+int grouped_device(int count, const b2_gemm_problem *problems, cudaStream_t s, int *info);
+int grouped_plan_create(int count, const b2_gemm_problem *problems, void **plan, int *info);
+int grouped_plan_launch(void *plan, cudaStream_t s);
+int grouped_plan_destroy(void *plan);
+
 // 3M complex GEMM, one fused launch (gemm3m.cu); alpha/beta are (re, im) pairs.
 template <typename T>
 int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T *A, int lda,

@@ -1,0 +1,341 @@
+// grouped.cu -- thousands of independent GEMMs in one persistent launch.
+//
+// The reference parallelises one GEMM at a time: a static N split over OpenMP
+// threads (src/gemm_driver.c:136-149) or a CAS task queue of 192 x (96 k)
+// tiles (OpenBLAS-like_implementation/dgemm.c:449-483, get_gemm_task).  The
+// B200 form of that queue runs across a whole batch of unrelated problems:
+// the host flattens every problem into 64 x 64 output tiles (problems sorted
+// by K, largest first, so the longest tiles are handed out first), a
+// persistent grid pulls tile indices from a device-side atomic counter, finds
+// the owning problem by binary search over the tile prefix sums and runs the
+// tile with the problem's own dtype, transposes, strides and alpha/beta:
+//   FP64 tiles: DMMA mma.sync.m16n8k4.f64, 8 warps of 32 x 16;
+//   FP32 tiles: FFMA, 256 threads of 4 x 4.
+// A plan uploads the descriptors once and captures "reset counter + launch" in
+// a CUDA graph, so replaying a batch is a single graph launch.
+#include <stdlib.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "b2_methods.cuh"
+#include "b2_profile.cuh"
+
+namespace b2 {
+namespace {
+
+constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+constexpr int GT_LD = GT_M + 4;  // [k][m] stride (68 = 4 mod 16 doubles)
+
+struct GroupDesc {
+  const void *A;
+  const void *B;
+  void *C;
+  double alpha, beta;
+  int m, n, k, lda, ldb, ldc;
+  int dtype;  // 0 = f64, 1 = f32
+  int ta, tb;
+  int tiles_m, tiles_n;
+  long long tile_offset;
+};
+
+// Stage a GT_K-deep panel: op(A) tile (64 x 16) and op(B) tile (16 x 64) into
+// shared memory as As[k][m] and Bs[k][n] (stride GT_LD), zero outside.
+template <typename T>
+__device__ __forceinline__ void stage_panel(const GroupDesc &g, int m0, int n0, int k0, T *As,
+                                            T *Bs) {
+  const T *A = (const T *)g.A;
+  const T *B = (const T *)g.B;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int idx = threadIdx.x + 256 * e;
+    int mm, kk;
+    if (g.ta) { kk = idx % GT_K; mm = idx / GT_K; } else { mm = idx % GT_M; kk = idx / GT_M; }
+    const int gm = m0 + mm, gk = k0 + kk;
+    T v = 0;
+    if (gm < g.m && gk < g.k)
+      v = g.ta ? A[(long long)gm * g.lda + gk] : A[(long long)gk * g.lda + gm];
+    As[kk * GT_LD + mm] = v;
+    int nn;
+    if (g.tb) { nn = idx % GT_N; kk = idx / GT_N; } else { kk = idx % GT_K; nn = idx / GT_K; }
+    const int gn = n0 + nn, gk2 = k0 + kk;
+    T w = 0;
+    if (gn < g.n && gk2 < g.k)
+      w = g.tb ? B[(long long)gk2 * g.ldb + gn] : B[(long long)gn * g.ldb + gk2];
+    Bs[kk * GT_LD + nn] = w;
+  }
+}
+
+__device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
+  double *As = sm, *Bs = sm + GT_K * GT_LD;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane >> 2, t = lane & 3;
+  const int wm0 = (warp >> 2) * 32, wn0 = (warp & 3) * 16;
+  double acc[2][2][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+  for (int k0 = 0; k0 < g.k; k0 += GT_K) {
+    __syncthreads();
+    stage_panel<double>(g, m0, n0, k0, As, Bs);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GT_K; kk += 4) {
+      double af[2][2], bf[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) af[i][v] = As[(kk + t) * GT_LD + wm0 + i * 16 + gq + 8 * v];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) bf[j] = Bs[(kk + t) * GT_LD + wn0 + j * 8 + gq];
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+          asm volatile(
+              "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+              "{%0,%1,%2,%3};\n"
+              : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
+              : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
+    }
+  }
+  double *C = (double *)g.C;
+  const bool one = (g.beta == 1.0);
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int m = m0 + wm0 + i * 16 + gq + 8 * (v >> 1);
+        const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
+        if (m < g.m && n < g.n) {
+          double *p = C + (long long)n * g.ldc + m;
+          *p = one ? fma(g.alpha, acc[i][j][v], *p) : fma(g.alpha, acc[i][j][v], g.beta * *p);
+        }
+      }
+}
+
+__device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
+  float *As = sm, *Bs = sm + GT_K * GT_LD;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  for (int k0 = 0; k0 < g.k; k0 += GT_K) {
+    __syncthreads();
+    stage_panel<float>(g, m0, n0, k0, As, Bs);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GT_K; ++kk) {
+      const float4 a = *reinterpret_cast<const float4 *>(&As[kk * GT_LD + tx * 4]);
+      const float4 b = *reinterpret_cast<const float4 *>(&Bs[kk * GT_LD + ty * 4]);
+      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+  }
+  float *C = (float *)g.C;
+  const float al = (float)g.alpha, be = (float)g.beta;
+  const bool one = (be == 1.f);
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int m = m0 + tx * 4 + i, n = n0 + ty * 4 + j;
+      if (m < g.m && n < g.n) {
+        float *p = C + (long long)n * g.ldc + m;
+        *p = one ? fmaf(al, acc[i][j], *p) : fmaf(al, acc[i][j], be * *p);
+      }
+    }
+}
+
+__global__ void __launch_bounds__(256)
+    grouped_kernel(const GroupDesc *__restrict__ d, int count, long long total_tiles,
+                   unsigned long long *counter) {
+  __shared__ __align__(16) double sm[2 * GT_K * GT_LD];
+  __shared__ long long tile_s;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) tile_s = (long long)atomicAdd(counter, 1ull);
+    __syncthreads();
+    const long long t = tile_s;
+    if (t >= total_tiles) break;
+    int lo = 0, hi = count - 1;  // last problem whose first tile <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (d[mid].tile_offset <= t) lo = mid; else hi = mid - 1;
+    }
+    const GroupDesc g = d[lo];
+    const int local = (int)(t - g.tile_offset);
+    const int m0 = (local % g.tiles_m) * GT_M, n0 = (local / g.tiles_m) * GT_N;
+    if (g.dtype == 0) tile_f64(g, m0, n0, sm);
+    else tile_f32(g, m0, n0, reinterpret_cast<float *>(sm));
+  }
+}
+
+struct Plan {
+  int device = -1;
+  int count = 0;
+  long long total_tiles = 0;
+  GroupDesc *d_desc = nullptr;
+  unsigned long long *d_counter = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int grid = 0;
+};
+
+bool is_nt(char c) { return c == 'N' || c == 'n'; }
+
+int build_descs(int count, const b2_gemm_problem *pr, std::vector<GroupDesc> &out,
+                long long *total, int *info) {
+  std::vector<int> order(count);
+  std::iota(order.begin(), order.end(), 0);
+  // largest K first: each tile costs ~K, so the long tiles are dequeued first
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return pr[a].k > pr[b].k; });
+  out.clear();
+  long long off = 0;
+  for (int idx : order) {
+    const b2_gemm_problem &p = pr[idx];
+    int inf = 0;
+    if (p.dtype != 0 && p.dtype != 1) { *info = idx + 1; return B2_ERR_ARG; }
+    if (check_gemm(p.transa, p.transb, p.m, p.n, p.k, p.lda, p.ldb, p.ldc, p.A, p.B, p.C, &inf) !=
+        B2_OK) {
+      *info = idx + 1;
+      return B2_ERR_ARG;
+    }
+    if (p.m == 0 || p.n == 0) continue;
+    GroupDesc g;
+    g.A = p.A;
+    g.B = p.B;
+    g.C = p.C;
+    g.alpha = p.alpha;
+    g.beta = p.beta;
+    g.m = p.m;
+    g.n = p.n;
+    g.k = p.k;
+    g.lda = p.lda;
+    g.ldb = p.ldb;
+    g.ldc = p.ldc;
+    g.dtype = p.dtype;
+    g.ta = is_nt(p.transa) ? 0 : 1;
+    g.tb = is_nt(p.transb) ? 0 : 1;
+    g.tiles_m = (p.m + GT_M - 1) / GT_M;
+    g.tiles_n = (p.n + GT_N - 1) / GT_N;
+    g.tile_offset = off;
+    off += (long long)g.tiles_m * g.tiles_n;
+    out.push_back(g);
+  }
+  *total = off;
+  return B2_OK;
+}
+
+int enqueue(const Plan &p, cudaStream_t s) {
+  B2_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned long long), s));
+  if (p.total_tiles == 0) return B2_OK;
+  B2_PROF("grouped_gemm", s);
+  grouped_kernel<<<p.grid, 256, 0, s>>>(p.d_desc, p.count, p.total_tiles, p.d_counter);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+void free_plan(Plan *p) {
+  if (!p) return;
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->d_desc) cudaFree(p->d_desc);
+  if (p->d_counter) cudaFree(p->d_counter);
+  delete p;
+}
+
+int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **out, int *info) {
+  Ctx *cx = ctx();
+  if (!cx) return B2_ERR_NO_DEVICE;
+  std::vector<GroupDesc> descs;
+  long long total = 0;
+  int rc = build_descs(count, problems, descs, &total, info);
+  if (rc != B2_OK) return rc;
+  Plan *p = new Plan();
+  p->device = cx->device;
+  p->count = (int)descs.size();
+  p->total_tiles = total;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, 256, 0);
+  if (per_sm < 1) per_sm = 1;
+  const long long want = (long long)cx->sm_count * per_sm;
+  p->grid = (int)(total < want ? (total > 0 ? total : 1) : want);
+  if (cudaMalloc(&p->d_desc, sizeof(GroupDesc) * (descs.empty() ? 1 : descs.size())) != cudaSuccess ||
+      cudaMalloc(&p->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    free_plan(p);
+    return B2_ERR_NOMEM;
+  }
+  if (!descs.empty() &&
+      cudaMemcpy(p->d_desc, descs.data(), sizeof(GroupDesc) * descs.size(),
+                 cudaMemcpyHostToDevice) != cudaSuccess) {
+    free_plan(p);
+    return cuda_fail(cudaGetLastError(), "grouped descriptors");
+  }
+  if (capture) {
+    cudaStream_t cs;
+    if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) {
+      free_plan(p);
+      return cuda_fail(cudaGetLastError(), "capture stream");
+    }
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      rc = enqueue(*p, cs);
+      e = cudaStreamEndCapture(cs, &p->graph);
+    }
+    if (e == cudaSuccess && rc == B2_OK) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess || rc != B2_OK) {
+      free_plan(p);
+      return rc != B2_OK ? rc : cuda_fail(e, "grouped graph capture");
+    }
+  }
+  *out = p;
+  return B2_OK;
+}
+
+}  // namespace
+
+int grouped_device(int count, const b2_gemm_problem *problems, cudaStream_t s, int *info) {
+  Plan *p = nullptr;
+  int rc = make_plan(count, problems, false, &p, info);
+  if (rc != B2_OK) return rc;
+  rc = enqueue(*p, s);
+  // the descriptor buffer must outlive the launch
+  cudaStreamSynchronize(s);
+  free_plan(p);
+  return rc;
+}
+
+int grouped_plan_create(int count, const b2_gemm_problem *problems, void **plan, int *info) {
+  Plan *p = nullptr;
+  const int rc = make_plan(count, problems, true, &p, info);
+  if (rc == B2_OK) *plan = p;
+  return rc;
+}
+
+int grouped_plan_launch(void *plan, cudaStream_t s) {
+  Plan *p = (Plan *)plan;
+  cudaError_t e = cudaGraphLaunch(p->exec, s);
+  if (e != cudaSuccess) return cuda_fail(e, "grouped graph launch");
+  return B2_OK;
+}
+
+int grouped_plan_destroy(void *plan) {
+  free_plan((Plan *)plan);
+  return B2_OK;
+}
+
+}  // namespace b2

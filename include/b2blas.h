@@ -177,6 +177,35 @@ B2_API int b2_cgemm3m(char transa, char transb, int m, int n, int k, const float
                const float *A, int lda, const float *B, int ldb, const float *beta, float *C,
                int ldc, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* Grouped GEMM: many independent problems in one persistent launch.  No     */
+/* counterpart API in the reference, whose parallel drivers split one GEMM   */
+/* (src/gemm_driver.c:136-149; OpenBLAS-like_implementation/dgemm.c:449-483   */
+/* task queue); here the queue spans a whole batch.  Pointers are device     */
+/* pointers; each problem follows the dgemm_/sgemm_ contract.                */
+/* ------------------------------------------------------------------------ */
+typedef struct b2_gemm_problem {
+  int dtype;            /* 0 = FP64 (double), 1 = FP32 (float) */
+  char transa, transb;  /* 'N'/'n' = no transpose, anything else = transpose */
+  int m, n, k;
+  double alpha, beta;   /* rounded to float for dtype 1 */
+  const void *A;
+  int lda;
+  const void *B;
+  int ldb;
+  void *C;
+  int ldc;
+} b2_gemm_problem;
+
+/* One-shot: upload descriptors, launch, wait for the descriptors to be consumed.
+ * On an invalid problem returns B2_ERR_ARG with b2_last_info() = its 1-based index. */
+B2_API int b2_gemm_grouped(int count, const b2_gemm_problem *problems, void *stream);
+/* Plan: descriptors uploaded once and "reset queue + launch" captured in a CUDA
+ * graph; b2_grouped_plan_launch replays it (one graph launch) on `stream`. */
+B2_API int b2_grouped_plan_create(int count, const b2_gemm_problem *problems, void **plan);
+B2_API int b2_grouped_plan_launch(void *plan, void *stream);
+B2_API int b2_grouped_plan_destroy(void *plan);
+
 /* Error statistics of C against a double-double reference computed on the
  * device from the same inputs: normwise ||C - Cdd||_F / ||Cdd||_F and
  * max_ij |C - Cdd| / max_ij |Cdd|.  Synchronous.  Allocates scratch. */
