@@ -100,6 +100,19 @@ def lib() -> C.CDLL:
     for nm in ("b2_gemm_grouped", "b2_grouped_plan_create", "b2_grouped_plan_launch",
                "b2_grouped_plan_destroy"):
         getattr(L, nm).restype = i
+    L.b2_tune_config_count.restype = i
+    L.b2_mlp_param_count.restype = i
+    L.b2_dgemm_config.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, p]
+    L.b2_tune_sweep.argtypes = [i, p, i, p]
+    L.b2_mlp_train.argtypes = [i, p, p, i, i, f, i, p, p, p]
+    L.b2_mlp_forward.argtypes = [p, i, p, p]
+    L.b2_mlp_gradient.argtypes = [p, i, p, p, p, p]
+    L.b2_selector_set.argtypes = [p]
+    L.b2_selector_choose.argtypes = [ch, ch, i, i, i, i, i]
+    L.b2_selector_predict.argtypes = [ch, ch, i, i, i, i, p]
+    for nm in ("b2_dgemm_config", "b2_tune_sweep", "b2_mlp_train", "b2_mlp_forward",
+               "b2_mlp_gradient", "b2_selector_set", "b2_selector_choose", "b2_selector_predict"):
+        getattr(L, nm).restype = i
     L.b2_set_fp64_config.argtypes = [i, i, i]
     L.b2_set_fp64_config.restype = i
     L.b2_launch_count.restype = C.c_longlong

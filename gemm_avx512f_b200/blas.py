@@ -20,7 +20,7 @@ from ._lib import METHODS, B2Error, check, lib
 __all__ = [
     "dgemm", "sgemm", "dtrsm", "zgemm3m", "cgemm3m", "set_dgemm_method", "set_sgemm_method",
     "dgemm_device", "sgemm_device", "dgemm_dd_device", "dgemm_error_device", "dtrsm_device",
-    "zgemm3m_device", "cgemm3m_device", "last_error", "B2Error",
+    "zgemm3m_device", "cgemm3m_device", "last_error", "B2Error", "load_selector",
 ]
 
 
@@ -115,6 +115,22 @@ def cgemm3m(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
 
 def set_dgemm_method(method: str = "fp64", slices: int = 0) -> None:
     check(lib().b2_set_dgemm_method(METHODS[method], int(slices)), "b2_set_dgemm_method")
+
+
+def load_selector(path: str | None = None) -> bool:
+    """Install the learned configuration selector used by method="auto"
+    (default: the weights trained on B200 shipped in gemm_avx512f_b200/data)."""
+    import os
+
+    if path is None:
+        path = os.path.join(os.path.dirname(__file__), "data", "selector_nvidia_b200.f32")
+    if not os.path.exists(path):
+        return False
+    w = np.fromfile(path, np.float32)
+    if w.size != lib().b2_mlp_param_count():
+        raise ValueError(f"{path}: expected {lib().b2_mlp_param_count()} parameters, got {w.size}")
+    check(lib().b2_selector_set(w.ctypes.data), "b2_selector_set")
+    return True
 
 
 def set_sgemm_method(method: str = "fp32") -> None:

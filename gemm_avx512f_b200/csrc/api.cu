@@ -88,6 +88,15 @@ Ctx *ctx() {
   if (const char *s = getenv("B2_SLICES")) c->dgemm_slices = atoi(s);
   g_ctx = c;
   g_owner.c = c;
+  if (const char *path = getenv("B2_SELECTOR")) {  // learned selector weights for AUTO
+    if (FILE *fh = fopen(path, "rb")) {
+      const int np = b2_mlp_param_count();
+      float *w = (float *)malloc(sizeof(float) * np);
+      if (w && fread(w, sizeof(float), np, fh) == (size_t)np) b2_selector_set(w);
+      free(w);
+      fclose(fh);
+    }
+  }
   return c;
 }
 
@@ -173,7 +182,8 @@ int dgemm_device(char ta, char tb, int m, int n, int k, double alpha, const doub
   if (!c) return B2_ERR_NO_DEVICE;
   if (method == B2_METHOD_DEFAULT) method = c->dgemm_method;
   if (slices <= 0) slices = c->dgemm_slices;
-  if (method == B2_METHOD_AUTO) method = select_dgemm_method(c, ta, tb, m, n, k, &slices);
+  if (method == B2_METHOD_AUTO)
+    return dgemm_auto(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices, s);
   if (method == B2_METHOD_OZAKI)
     return dgemm_ozaki(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices, s);
   return dgemm_fp64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s, nullptr);

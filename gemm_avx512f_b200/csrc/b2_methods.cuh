@@ -23,14 +23,19 @@ int sgemm_device(char ta, char tb, int m, int n, int k, float alpha, const float
                  const float *B, int ldb, float beta, float *C, int ldc, int method,
                  cudaStream_t s);
 
-// Method selection for B2_METHOD_AUTO (selector.cu).
+// Method selection for B2_METHOD_AUTO (tuner.cu): configuration chosen by the
+// learned selector when installed, else by the measured heuristic.
 int select_dgemm_method(Ctx *c, char ta, char tb, int m, int n, int k, int *slices);
+int dgemm_auto(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+               const double *B, int ldb, double beta, double *C, int ldc, int slices,
+               cudaStream_t s);
 
 // INT8 Ozaki emulation of DGEMM (ozaki.cu).  slices = modulus count, 0 = auto.
 int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
                 const double *B, int ldb, double beta, double *C, int ldc, int slices,
                 cudaStream_t s);
 int ozaki_auto_moduli(int k);
+void ozaki_set_variant(int v);  // INT8 engine shape of the allocating path (0..2)
 
 // SGEMM methods (sgemm.cu).
 int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,

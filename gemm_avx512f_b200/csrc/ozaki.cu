@@ -66,11 +66,11 @@ __constant__ unsigned c_k32[OZ_MAX];  // 2^32 mod m
 __constant__ unsigned c_k48[OZ_MAX];  // 2^48 mod m
 __constant__ unsigned c_off[OZ_MAX];  // m - (2^62 mod m): undoes the +2^62 offset
 __constant__ unsigned c_magic[OZ_MAX];  // floor(2^32 / m) + 1 (Barrett)
-__constant__ double c_Wd[OZ_MAX][4];  // CRT weights in 32-bit limbs (low first)
-__constant__ double c_Pd[4];          // P in 32-bit limbs
-__constant__ long long c_W[OZ_MAX][3];
-__constant__ long long c_P[3];
-__constant__ double c_invP;
+// CRT tables for every modulus count s = 0..OZ_MAX (index s), uploaded once per
+// device so calls with different counts never re-upload or synchronise.
+__constant__ double c_Wd[OZ_MAX + 1][OZ_MAX][4];  // weights in 32-bit limbs (low first)
+__constant__ double c_Pd[OZ_MAX + 1][4];          // P in 32-bit limbs
+__constant__ double c_invP[OZ_MAX + 1];
 
 typedef unsigned __int128 u128;
 
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(256)
       for (int e = 0; e < 4; ++e) {
         const double rd = byte_to_double((w4 >> (8 * e)) & 0xFFu);
 #pragma unroll
-        for (int l = 0; l < 4; ++l) S[e][l] = fma(rd, c_Wd[i][l], S[e][l]);
+        for (int l = 0; l < 4; ++l) S[e][l] = fma(rd, c_Wd[s][i][l], S[e][l]);
       }
     }
     const int tg = tauB[n];
@@ -401,11 +401,11 @@ __global__ void __launch_bounds__(256)
       } else {
         const double Sd =
             fma(S[e][3], 0x1p96, fma(S[e][2], 0x1p64, fma(S[e][1], 0x1p32, S[e][0])));
-        const double q = rint(Sd * c_invP);
-        long long X0 = __double2ll_rn(fma(-q, c_Pd[0], S[e][0]));
-        long long X1 = __double2ll_rn(fma(-q, c_Pd[1], S[e][1]));
-        long long X2 = __double2ll_rn(fma(-q, c_Pd[2], S[e][2]));
-        long long X3 = __double2ll_rn(fma(-q, c_Pd[3], S[e][3]));
+        const double q = rint(Sd * c_invP[s]);
+        long long X0 = __double2ll_rn(fma(-q, c_Pd[s][0], S[e][0]));
+        long long X1 = __double2ll_rn(fma(-q, c_Pd[s][1], S[e][1]));
+        long long X2 = __double2ll_rn(fma(-q, c_Pd[s][2], S[e][2]));
+        long long X3 = __double2ll_rn(fma(-q, c_Pd[s][3], S[e][3]));
         long long cy = X0 >> 32;
         X0 -= cy << 32;
         X1 += cy;
@@ -429,12 +429,15 @@ struct OzPlan {
   int s = 0, kchunks = 0;
 };
 thread_local OzPlan g_last_plan;
-thread_local int g_table_s = -1;
-thread_local int g_table_dev = -1;
 
-int upload_table(int s, int dev, cudaStream_t st) {
-  if (g_table_s == s && g_table_dev == dev) return B2_OK;
-  const CrtTable t = make_table(s);
+std::mutex g_table_mu;
+bool g_table_done[64] = {};
+
+// Upload every constant table once per device (all modulus counts at once).
+int upload_tables(int dev, cudaStream_t st) {
+  if (dev < 0 || dev >= 64) return B2_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lk(g_table_mu);
+  if (g_table_done[dev]) return B2_OK;
   int mod[OZ_MAX];
   float invf[OZ_MAX];
   double invd[OZ_MAX];
@@ -449,6 +452,16 @@ int upload_table(int s, int dev, cudaStream_t st) {
     off[i] = (unsigned)(kModuli[i] - (int)((1ull << 62) % (unsigned long long)kModuli[i]));
     magic[i] = (unsigned)((1ull << 32) / (unsigned long long)kModuli[i] + 1);
   }
+  static double wd[OZ_MAX + 1][OZ_MAX][4], pd[OZ_MAX + 1][4], ip[OZ_MAX + 1];
+  memset(wd, 0, sizeof(wd));
+  memset(pd, 0, sizeof(pd));
+  memset(ip, 0, sizeof(ip));
+  for (int s = 2; s <= OZ_MAX; ++s) {
+    const CrtTable t = make_table(s);
+    memcpy(wd[s], t.Wd, sizeof(t.Wd));
+    memcpy(pd[s], t.Pd, sizeof(t.Pd));
+    ip[s] = t.invP;
+  }
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_mod, mod, sizeof(mod), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invf, invf, sizeof(invf), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invd, invd, sizeof(invd), 0, cudaMemcpyHostToDevice, st));
@@ -457,20 +470,41 @@ int upload_table(int s, int dev, cudaStream_t st) {
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k48, k48, sizeof(k48), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_off, off, sizeof(off), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_magic, magic, sizeof(magic), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Wd, t.Wd, sizeof(t.Wd), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Pd, t.Pd, sizeof(t.Pd), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_W, t.W, sizeof(t.W), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_P, t.Pl, sizeof(t.Pl), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invP, &t.invP, sizeof(double), 0, cudaMemcpyHostToDevice, st));
-  // The constant bank is shared by every stream: finish the upload before any
-  // other stream can launch against it.
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Wd, wd, sizeof(wd), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Pd, pd, sizeof(pd), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invP, ip, sizeof(ip), 0, cudaMemcpyHostToDevice, st));
+  // The constant bank is shared by every stream: finish before any launch uses it.
   B2_CUDA_TRY(cudaStreamSynchronize(st));
-  g_table_s = s;
-  g_table_dev = dev;
+  g_table_done[dev] = true;
   return B2_OK;
 }
 
 inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
+
+// INT8 engine shape used by the allocating Ozaki path (tuning variants):
+//   0: 128 x 256 tile, 4 stages   1: 128 x 128 tile, 6 stages   2: 128 x 128, 4 stages
+thread_local int g_oz_variant = 0;
+
+int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, int n, int m, int s,
+                long long kp, long long planeX, long long planeY, const ResidueEpi &epi,
+                int sm_count, int *derr, cudaStream_t st) {
+  const int bn = variant == 0 ? 256 : 128;
+  CUtensorMap tmX, tmY;
+  int rc = umma::make_kmajor_map(&tmX, umma::KIND_I8, X, kcl, n, s, kp, planeX, umma::BM);
+  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, kcl, m, s, kp, planeY, bn);
+  if (rc != B2_OK) return rc;
+  switch (variant) {
+    case 1:
+      return umma::launch<umma::KIND_I8, 128, 6>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
+                                                  "ozaki_i8_gemm");
+    case 2:
+      return umma::launch<umma::KIND_I8, 128, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
+                                                  "ozaki_i8_gemm");
+    default:
+      return umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
+                                                  "ozaki_i8_gemm");
+  }
+}
 
 // Exponents for the R "rows" of an operand (element (r,k) at X[r*sr + k*sk]).
 // K chunks of the norm pass: about one per 1024 of K, more when there are few
@@ -517,6 +551,8 @@ size_t norm_scratch_bytes(int R, int K) {
 
 }  // namespace
 
+void ozaki_set_variant(int v) { g_oz_variant = (v >= 0 && v <= 2) ? v : 0; }
+
 int ozaki_auto_moduli(int k) {
   // Both the truncation error (~2^-H sqrt(K)) and FP64 rounding (~u sqrt(K))
   // grow like sqrt(K) relative to |C|, so the count that matches FP64 does not
@@ -539,7 +575,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   if (k <= 0 || alpha == 0.0) return beta == 1.0 ? B2_OK : scale_matrix_d(m, n, beta, C, ldc, st);
   const int s = slices > 0 ? slices : ozaki_auto_moduli(k);
   if (s < 2 || s > OZ_MAX) return B2_ERR_ARG;
-  int rc = upload_table(s, cx->device, st);
+  int rc = upload_tables(cx->device, st);
   if (rc != B2_OK) return rc;
   const CrtTable t = make_table(s);
 
@@ -593,13 +629,9 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
         slice_kernel<false><<<grid, 256, 0, st>>>(B + kc0 * bsk, bsr, bsk, n, kcl, tauB, s, X, kp, planeX);
       B2_CUDA_TRY(cudaGetLastError());
     }
-    CUtensorMap tmX, tmY;
-    rc = umma::make_kmajor_map(&tmX, umma::KIND_I8, X, kcl, n, s, kp, planeX, umma::BM);
-    if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, kcl, m, s, kp, planeY, 256);
-    if (rc != B2_OK) return rc;
     ResidueEpi epi{Rb, planeR, (int)mp, n, m, c > 0 ? 1 : 0};
-    rc = umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, kcl, s, epi, cx->sm_count, cx->derr,
-                                              st, "ozaki_i8_gemm");
+    rc = run_i8_gemm(g_oz_variant, X, Y, kcl, n, m, s, kp, planeX, planeY, epi, cx->sm_count,
+                     cx->derr, st);
   }
   if (rc != B2_OK) return rc;
   {
@@ -731,7 +763,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   // the error word is the only state that must start at zero
   B2_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), st));
 
-  rc = upload_table(s, dev, st);
+  rc = upload_tables(dev, st);
   if (rc != B2_OK) return rc;
   const CrtTable t = make_table(s);
   const bool tA = !(transa == 'N' || transa == 'n');

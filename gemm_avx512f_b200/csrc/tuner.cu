@@ -1,0 +1,302 @@
+// tuner.cu -- DGEMM configuration space, exhaustive timing sweep, and the
+// learned selector's per-call inference.
+//
+// Replaces the reference's compile-time tuning (dgemm_tune.h:6-15,
+// sgemm_tune.h:6-15 clamped by src/gemm_set_parameters.h:10-82: unroll and
+// loop counts fixed per CPU model) with run-time choices made per shape:
+//
+//   config  0..35  plain FP64 DMMA: tile {128x128, 128x64, 64x64}
+//                  x DMMA K shape {4, 8, 16} x split-K {1, 2, 4, 8}
+//   config 36..47  INT8 Ozaki emulation: moduli {13, 14, 15, 16}
+//                  x INT8 engine shape {128x256/4 stages, 128x128/6, 128x128/4}
+//
+// b2_tune_sweep times every configuration of every shape (minimum of `reps`
+// CUDA-event timings of back-to-back batches, inputs resident), the
+// exhaustive autotuner whose timing
+// database trains the MLP selector (mlp.cu).  With selector weights installed,
+// B2_METHOD_AUTO runs a 7-64-64-48 ReLU MLP on the host per call (a few
+// microseconds) and takes the fastest predicted configuration among those
+// that meet the accuracy rule (Ozaki only with >= the required moduli).
+#include <math.h>
+#include <string.h>
+
+#include <mutex>
+#include <vector>
+
+#include "b2_methods.cuh"
+#include "b2_profile.cuh"
+
+namespace b2 {
+
+constexpr int NCFG = 48;
+constexpr int MLP_IN = 7, MLP_H = 64, MLP_OUT = NCFG;
+constexpr int MLP_PARAMS =
+    MLP_IN * MLP_H + MLP_H + MLP_H * MLP_H + MLP_H + MLP_H * MLP_OUT + MLP_OUT;
+
+struct TuneCfg {
+  int method;
+  Fp64Cfg f;
+  int slices;
+  int variant;
+};
+
+TuneCfg decode_cfg(int idx) {
+  static const int mmaks[3] = {4, 8, 16};
+  TuneCfg c{};
+  if (idx < 36) {
+    c.method = B2_METHOD_FP64;
+    c.f.tile = idx / 12;
+    c.f.mmak = mmaks[(idx / 4) % 3];
+    c.f.split_k = 1 << (idx % 4);
+  } else {
+    const int j = idx - 36;
+    c.method = B2_METHOD_OZAKI;
+    c.slices = 13 + j / 3;
+    c.variant = j % 3;
+  }
+  return c;
+}
+
+int run_config(int idx, char ta, char tb, int m, int n, int k, double alpha, const double *A,
+               int lda, const double *B, int ldb, double beta, double *C, int ldc,
+               cudaStream_t s) {
+  const TuneCfg c = decode_cfg(idx);
+  if (c.method == B2_METHOD_FP64)
+    return dgemm_fp64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s, &c.f);
+  ozaki_set_variant(c.variant);
+  const int rc = dgemm_ozaki(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c.slices, s);
+  ozaki_set_variant(0);
+  return rc;
+}
+
+// Features of a call: log2 sizes centred on 2^7 and scaled by 1/3, transposes,
+// dtype (0 = FP64), beta == 0.
+void mlp_features(char ta, char tb, int m, int n, int k, int dtype, int beta0, float *x) {
+  x[0] = (float)((log2((double)(m > 0 ? m : 1)) - 7.0) / 3.0);
+  x[1] = (float)((log2((double)(n > 0 ? n : 1)) - 7.0) / 3.0);
+  x[2] = (float)((log2((double)(k > 0 ? k : 1)) - 7.0) / 3.0);
+  x[3] = (ta == 'N' || ta == 'n') ? 0.f : 1.f;
+  x[4] = (tb == 'N' || tb == 'n') ? 0.f : 1.f;
+  x[5] = (float)dtype;
+  x[6] = beta0 ? 1.f : 0.f;
+}
+
+// Host forward pass (same parameter layout as the CUDA kernels in mlp.cu:
+// W1[in][64], b1, W2[64][64], b2, W3[64][48], b3).
+void mlp_forward_host(const float *w, const float *x, float *y) {
+  const float *W1 = w, *b1 = W1 + MLP_IN * MLP_H, *W2 = b1 + MLP_H, *b2 = W2 + MLP_H * MLP_H;
+  const float *W3 = b2 + MLP_H, *b3 = W3 + MLP_H * MLP_OUT;
+  float h1[MLP_H], h2[MLP_H];
+  for (int o = 0; o < MLP_H; ++o) {
+    float a = b1[o];
+    for (int i = 0; i < MLP_IN; ++i) a += x[i] * W1[i * MLP_H + o];
+    h1[o] = a > 0.f ? a : 0.f;
+  }
+  for (int o = 0; o < MLP_H; ++o) {
+    float a = b2[o];
+    for (int i = 0; i < MLP_H; ++i) a += h1[i] * W2[i * MLP_H + o];
+    h2[o] = a > 0.f ? a : 0.f;
+  }
+  for (int o = 0; o < MLP_OUT; ++o) {
+    float a = b3[o];
+    for (int i = 0; i < MLP_H; ++i) a += h2[i] * W3[i * MLP_OUT + o];
+    y[o] = a;
+  }
+}
+
+namespace {
+std::mutex g_sel_mu;
+std::vector<float> g_sel_w;  // empty: no learned selector installed
+}  // namespace
+
+bool cfg_allowed(int idx, int min_slices) {
+  return idx < 36 || decode_cfg(idx).slices >= min_slices;
+}
+
+// Choice used when no selector is installed or the shape lies outside the
+// trained range (any dimension > 2048): plain FP64 with the measured default
+// tile, the INT8 emulation (required moduli, 128x256 engine) once every
+// dimension reaches 4096 (measured crossover region on B200).
+int heuristic_cfg(int m, int n, int k, int min_slices, int sm_count) {
+  if (m >= 4096 && n >= 4096 && k >= 4096 && min_slices >= 13 && min_slices <= 16)
+    return 36 + (min_slices - 13) * 3;
+  const Fp64Cfg f = fp64_default_cfg(m, n, k, sm_count);
+  const int mi = f.mmak == 4 ? 0 : f.mmak == 8 ? 1 : 2;
+  int sk = 0;
+  while ((1 << sk) < f.split_k && sk < 3) ++sk;
+  return f.tile * 12 + mi * 4 + sk;
+}
+
+int select_cfg(char ta, char tb, int m, int n, int k, int beta0, int min_slices, int sm_count) {
+  std::vector<float> w;
+  {
+    std::lock_guard<std::mutex> lk(g_sel_mu);
+    w = g_sel_w;
+  }
+  if (w.empty() || m > 2048 || n > 2048 || k > 2048) return heuristic_cfg(m, n, k, min_slices, sm_count);
+  float x[MLP_IN], y[MLP_OUT];
+  mlp_features(ta, tb, m, n, k, 0, beta0, x);
+  mlp_forward_host(w.data(), x, y);
+  int best = -1;
+  for (int c = 0; c < NCFG; ++c)
+    if (cfg_allowed(c, min_slices) && (best < 0 || y[c] < y[best])) best = c;
+  return best;
+}
+
+int select_dgemm_method(Ctx *c, char ta, char tb, int m, int n, int k, int *slices) {
+  const int need = *slices > 0 ? *slices : ozaki_auto_moduli(k);
+  const int cfg = select_cfg(ta, tb, m, n, k, 0, need, c->sm_count);
+  const TuneCfg t = decode_cfg(cfg);
+  *slices = t.method == B2_METHOD_OZAKI ? t.slices : 0;
+  return t.method;
+}
+
+int dgemm_auto(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
+               const double *B, int ldb, double beta, double *C, int ldc, int slices,
+               cudaStream_t s) {
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  const int need = slices > 0 ? slices : ozaki_auto_moduli(k);
+  const int cfg = select_cfg(ta, tb, m, n, k, beta == 0.0, need, c->sm_count);
+  return run_config(cfg, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+}
+
+namespace {
+__global__ void fill_uniform_kernel(double *x, long long n, unsigned long long seed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    x[i] = (double)(z >> 11) * 0x1p-52 - 1.0;  // U[-1, 1)
+  }
+}
+}  // namespace
+
+}  // namespace b2
+
+using namespace b2;
+
+extern "C" {
+
+int b2_tune_config_count(void) { return NCFG; }
+int b2_mlp_param_count(void) { return MLP_PARAMS; }
+
+int b2_dgemm_config(char transa, char transb, int m, int n, int k, double alpha, const double *A,
+                    int lda, const double *B, int ldb, double beta, double *C, int ldc,
+                    int config, void *stream) {
+  int info = 0;
+  if (config < 0 || config >= NCFG) return B2_ERR_ARG;
+  int st = check_gemm(transa, transb, m, n, k, lda, ldb, ldc, A, B, C, &info);
+  if (st != B2_OK) return st;
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  return run_config(config, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                    pick_stream(c, stream));
+}
+
+int b2_tune_sweep(int nshapes, const int *shapes, int reps, float *out_ms) {
+  if (nshapes < 0 || (nshapes > 0 && (!shapes || !out_ms)) || reps < 1) return B2_ERR_ARG;
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  long long ma = 1, mb = 1, mc = 1;
+  for (int i = 0; i < nshapes; ++i) {
+    const long long m = shapes[6 * i], n = shapes[6 * i + 1], k = shapes[6 * i + 2];
+    if (m < 1 || n < 1 || k < 1) return B2_ERR_ARG;
+    ma = ma > m * k ? ma : m * k;
+    mb = mb > k * n ? mb : k * n;
+    mc = mc > m * n ? mc : m * n;
+  }
+  double *A = nullptr, *B = nullptr, *C = nullptr;
+  cudaEvent_t e0, e1;
+  if (cudaMalloc(&A, ma * 8) != cudaSuccess || cudaMalloc(&B, mb * 8) != cudaSuccess ||
+      cudaMalloc(&C, mc * 8) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(A);
+    cudaFree(B);
+    cudaFree(C);
+    return B2_ERR_NOMEM;
+  }
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaStream_t s = c->stream;
+  fill_uniform_kernel<<<1024, 256, 0, s>>>(A, ma, 1);
+  fill_uniform_kernel<<<1024, 256, 0, s>>>(B, mb, 2);
+  fill_uniform_kernel<<<1024, 256, 0, s>>>(C, mc, 3);
+  int rc = B2_OK;
+  for (int i = 0; i < nshapes && rc == B2_OK; ++i) {
+    const int m = shapes[6 * i], n = shapes[6 * i + 1], k = shapes[6 * i + 2];
+    const char ta = shapes[6 * i + 3] ? 'T' : 'N', tb = shapes[6 * i + 4] ? 'T' : 'N';
+    const double beta = shapes[6 * i + 5] ? 0.0 : 1.0;
+    const int lda = ta == 'N' ? m : k, ldb = tb == 'N' ? k : n;
+    for (int cfg = 0; cfg < NCFG && rc == B2_OK; ++cfg) {
+      // One timed call sizes a batch of back-to-back calls (~100 us per
+      // timing, at most 32 calls): short calls are timed as the per-call
+      // average of a batch, which removes most of the event/launch jitter
+      // that dominates single timings of a few microseconds.
+      float single = 0.f;
+      cudaEventRecord(e0, s);
+      rc = run_config(cfg, ta, tb, m, n, k, 1.0, A, lda, B, ldb, beta, C, m, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "sweep");
+      cudaEventElapsedTime(&single, e0, e1);
+      int batch = single > 0.f ? (int)(0.1f / single) : 32;
+      batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
+      float best = 1e30f;
+      for (int r = 0; r < reps && rc == B2_OK; ++r) {
+        cudaEventRecord(e0, s);
+        for (int b = 0; b < batch && rc == B2_OK; ++b)
+          rc = run_config(cfg, ta, tb, m, n, k, 1.0, A, lda, B, ldb, beta, C, m, s);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "sweep");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)batch;
+        if (ms < best) best = ms;
+      }
+      out_ms[(long long)i * NCFG + cfg] = best;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(C);
+  return rc;
+}
+
+int b2_selector_set(const float *weights) {
+  std::lock_guard<std::mutex> lk(g_sel_mu);
+  if (!weights) {
+    g_sel_w.clear();
+  } else {
+    g_sel_w.assign(weights, weights + MLP_PARAMS);
+  }
+  return B2_OK;
+}
+
+int b2_selector_choose(char transa, char transb, int m, int n, int k, int beta_zero,
+                       int min_slices) {
+  Ctx *c = ctx();
+  const int sms = c ? c->sm_count : 148;
+  if (m < 1 || n < 1 || k < 1) return -1;
+  return select_cfg(transa, transb, m, n, k, beta_zero, min_slices > 0 ? min_slices : 15, sms);
+}
+
+int b2_selector_predict(char transa, char transb, int m, int n, int k, int beta_zero,
+                        float *pred) {
+  std::vector<float> w;
+  {
+    std::lock_guard<std::mutex> lk(g_sel_mu);
+    w = g_sel_w;
+  }
+  if (w.empty() || !pred) return B2_ERR_ARG;
+  float x[MLP_IN];
+  mlp_features(transa, transb, m, n, k, 0, beta_zero, x);
+  mlp_forward_host(w.data(), x, pred);
+  return B2_OK;
+}
+
+}  // extern "C"

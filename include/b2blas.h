@@ -231,6 +231,44 @@ B2_API int b2_device_error(int clear);
  * override (the selector decides again). */
 B2_API int b2_set_fp64_config(int tile, int mmak, int split_k);
 
+/* DGEMM configuration space of the autotuner: b2_tune_config_count() (= 48)
+ * configurations; 0..35 plain FP64 DMMA (tile {128x128,128x64,64x64} x DMMA K
+ * {4,8,16} x split-K {1,2,4,8}), 36..47 INT8 Ozaki (moduli {13..16} x INT8
+ * engine shape {128x256/4 stages, 128x128/6, 128x128/4}). */
+B2_API int b2_tune_config_count(void);
+/* Run one DGEMM (device pointers) with a given configuration. */
+B2_API int b2_dgemm_config(char transa, char transb, int m, int n, int k, double alpha,
+                           const double *A, int lda, const double *B, int ldb, double beta,
+                           double *C, int ldc, int config, void *stream);
+/* Exhaustive autotuner: shapes[6*i..] = {m, n, k, transA, transB, beta_is_zero};
+ * out_ms[48*i + c] = per-call time of configuration c, the fastest of `reps`
+ * CUDA-event timings of a batch of back-to-back calls (batch sized to ~100 us,
+ * at most 32 calls) on resident random inputs.  Synchronous; allocates its own
+ * buffers. */
+B2_API int b2_tune_sweep(int nshapes, const int *shapes, int reps, float *out_ms);
+
+/* Learned selector: a 7-64-64-48 ReLU MLP predicting log2(ms) per
+ * configuration from (log2 M, log2 N, log2 K centred at 7 and scaled by 1/3,
+ * transA, transB, dtype, beta == 0).  b2_mlp_param_count() floats, layout
+ * W1[7][64] b1 W2[64][64] b2 W3[64][48] b3.  Training, gradients and batched
+ * inference run in this library's own CUDA kernels. */
+B2_API int b2_mlp_param_count(void);
+B2_API int b2_mlp_train(int n, const float *X, const float *T, int epochs, int batch, float lr,
+                        int seed, const float *weights_in, float *weights_out,
+                        float *final_loss);
+B2_API int b2_mlp_forward(const float *weights, int n, const float *X, float *Y);
+B2_API int b2_mlp_gradient(const float *weights, int n, const float *X, const float *T,
+                           float *loss, float *grad);
+/* Install (or clear with NULL) the selector weights used by B2_METHOD_AUTO;
+ * b2_selector_choose returns the configuration AUTO would run (Ozaki
+ * configurations only with >= min_slices moduli), b2_selector_predict the 48
+ * predictions. */
+B2_API int b2_selector_set(const float *weights);
+B2_API int b2_selector_choose(char transa, char transb, int m, int n, int k, int beta_zero,
+                              int min_slices);
+B2_API int b2_selector_predict(char transa, char transb, int m, int n, int k, int beta_zero,
+                               float *pred);
+
 /* ------------------------------------------------------------------------ */
 /* Tracing (no counterpart in the reference, whose only instrumentation is   */
 /* the tester's clock_gettime loops, dtrsm_kernel_16x4_tester.c:267-287)     */
