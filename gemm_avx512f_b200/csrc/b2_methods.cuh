@@ -35,7 +35,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                 const double *B, int ldb, double beta, double *C, int ldc, int slices,
                 cudaStream_t s);
 int ozaki_auto_moduli(int k);
-void ozaki_set_variant(int v);  // INT8 engine shape of the allocating path (0..2)
+void ozaki_set_variant(int v);  // INT8 engine shape of the allocating path (0..4; -1 = default)
 
 // SGEMM methods (sgemm.cu).
 int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,

@@ -28,6 +28,7 @@
 // grows by ~4 bits per added modulus.  Rows or columns holding Inf/NaN are
 // computed by a direct FP64 dot product so IEEE propagation is kept.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <mutex>
@@ -483,15 +484,27 @@ inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a
 
 // INT8 engine shape used by the allocating Ozaki path (tuning variants):
 //   0: 128 x 256 tile, 4 stages   1: 128 x 128 tile, 6 stages   2: 128 x 128, 4 stages
-thread_local int g_oz_variant = 0;
+//   3: CTA pair, 256 x 256 tile, 6 stages   4: CTA pair, 256 x 256 tile, 7 stages
+// Default 3 (measured fastest at 8192^3 x 15 moduli: 124.5 vs 117.1 TFLOPS for
+// the whole Ozaki DGEMM with engine 0); B2_OZAKI_ENGINE (0..4) overrides it.
+constexpr int OZ_VARIANTS = 5;
+int default_oz_variant() {
+  static const int v = [] {
+    const char *e = getenv("B2_OZAKI_ENGINE");
+    const int x = e ? atoi(e) : 3;
+    return (x >= 0 && x < OZ_VARIANTS) ? x : 3;
+  }();
+  return v;
+}
+thread_local int g_oz_variant = default_oz_variant();
 
 int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, int n, int m, int s,
                 long long kp, long long planeX, long long planeY, const ResidueEpi &epi,
-                int sm_count, int *derr, cudaStream_t st) {
-  const int bn = variant == 0 ? 256 : 128;
+                int device, int sm_count, int *derr, cudaStream_t st) {
+  const int ybox = variant == 0 ? 256 : 128;  // pair variants stage BN/2 = 128 rows per CTA
   CUtensorMap tmX, tmY;
   int rc = umma::make_kmajor_map(&tmX, umma::KIND_I8, X, kcl, n, s, kp, planeX, umma::BM);
-  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, kcl, m, s, kp, planeY, bn);
+  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, kcl, m, s, kp, planeY, ybox);
   if (rc != B2_OK) return rc;
   switch (variant) {
     case 1:
@@ -500,6 +513,12 @@ int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, in
     case 2:
       return umma::launch<umma::KIND_I8, 128, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
                                                   "ozaki_i8_gemm");
+    case 3:
+      return umma::launch_pair<umma::KIND_I8, 256, 6>(tmX, tmY, n, m, kcl, s, epi, device, derr,
+                                                       st, "ozaki_i8_gemm");
+    case 4:
+      return umma::launch_pair<umma::KIND_I8, 256, 7>(tmX, tmY, n, m, kcl, s, epi, device, derr,
+                                                       st, "ozaki_i8_gemm");
     default:
       return umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
                                                   "ozaki_i8_gemm");
@@ -551,7 +570,9 @@ size_t norm_scratch_bytes(int R, int K) {
 
 }  // namespace
 
-void ozaki_set_variant(int v) { g_oz_variant = (v >= 0 && v <= 2) ? v : 0; }
+void ozaki_set_variant(int v) {
+  g_oz_variant = (v >= 0 && v < OZ_VARIANTS) ? v : default_oz_variant();
+}
 
 int ozaki_auto_moduli(int k) {
   // Both the truncation error (~2^-H sqrt(K)) and FP64 rounding (~u sqrt(K))
@@ -630,8 +651,8 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
       B2_CUDA_TRY(cudaGetLastError());
     }
     ResidueEpi epi{Rb, planeR, (int)mp, n, m, c > 0 ? 1 : 0};
-    rc = run_i8_gemm(g_oz_variant, X, Y, kcl, n, m, s, kp, planeX, planeY, epi, cx->sm_count,
-                     cx->derr, st);
+    rc = run_i8_gemm(g_oz_variant, X, Y, kcl, n, m, s, kp, planeX, planeY, epi, cx->device,
+                     cx->sm_count, cx->derr, st);
   }
   if (rc != B2_OK) return rc;
   {

@@ -65,7 +65,7 @@ int run_config(int idx, char ta, char tb, int m, int n, int k, double alpha, con
     return dgemm_fp64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s, &c.f);
   ozaki_set_variant(c.variant);
   const int rc = dgemm_ozaki(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, c.slices, s);
-  ozaki_set_variant(0);
+  ozaki_set_variant(-1);  // back to the default engine
   return rc;
 }
 

@@ -383,6 +383,297 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
+// ------------------------------------------------- CTA-pair (cta_group::2) --
+// The same product on a cluster of two CTAs that execute one 256 x BN MMA
+// together (tcgen05.mma.cta_group::2): CTA r of the pair stages X rows
+// [256 tp + 128 r, +128) and Y rows [BN tq + (BN/2) r, +BN/2) of every
+// K-block in its own shared memory, and the even ("leader") CTA issues the
+// MMAs, which read both CTAs' tiles and leave rows 128 r.. of the 256 x BN
+// accumulator in CTA r's TMEM.  Per MMA each SM loads a third less operand
+// data than the single-CTA 128 x 256 tile (32 KB vs 48 KB per K-block), which
+// is what keeps the tensor pipe fed from L2.
+//
+// Protocol (all loads are plain per-CTA TMA loads; none is multicast):
+//   full[s]   only the leader's is used: its producer posts expect_tx for both
+//             CTAs' bytes, and both CTAs' loads complete_tx on it (the
+//             .cta_group::2 load form with the leader's barrier address).
+//   empty[s]  one per CTA; the leader's commit arrives on both (commit
+//             multicast to the pair).
+//   tfull[a]  one per CTA; the leader's commit arrives on both.
+//   tempty[a] only the leader's is used: 8 arrivals, the 4 epilogue warps of
+//             each CTA (remote arrive from the odd CTA).
+// A timeout in either CTA raises the abort flag of both.  The pair meets in a
+// cluster barrier before TMEM is freed, so no MMA of the leader can still be
+// writing the odd CTA's TMEM, and neither CTA leaves while the other's copies
+// may still signal its barriers.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_id_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_count_x() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+  return r;
+}
+// Address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t map_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr)
+               : "memory");
+}
+__device__ __forceinline__ void st_cluster_u32(uint32_t cluster_addr, uint32_t v) {
+  asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(cluster_addr), "r"(v) : "memory");
+}
+// Per-CTA load into this CTA's shared memory, completing on a barrier that may
+// be the peer's (the pair form of the bulk tensor copy; no multicast).
+__device__ __forceinline__ void tma_load_3d_pair(uint32_t dst, const CUtensorMap *map,
+                                                 uint32_t bar_cluster, int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar_cluster), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+// Arrive (once the pair's MMAs issued so far complete) on the barrier at the
+// same offset in every CTA named by `mask`.
+__device__ __forceinline__ void tc_commit_pair(uint32_t bar, uint16_t mask) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(bar),
+      "h"(mask)
+      : "memory");
+}
+template <int KIND>
+__device__ __forceinline__ void tc_mma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                            uint32_t idesc, uint32_t accumulate) {
+  if constexpr (KIND == KIND_I8) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else if constexpr (KIND == KIND_BF16) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  }
+}
+
+// Bounded wait that also raises the peer CTA's abort flag on a timeout.
+__device__ __forceinline__ bool mbar_wait_pair(uint32_t bar, uint32_t parity,
+                                               volatile int *abort_flag, uint32_t peer_abort,
+                                               int *derr) {
+  if (mbar_wait(bar, parity, abort_flag, derr)) return true;
+  st_cluster_u32(peer_abort, 1u);
+  return false;
+}
+
+constexpr int PAIR_BM = 2 * BM;  // output rows per pair tile
+
+template <int KIND, int BN, int STAGES, class Epi>
+__global__ void __launch_bounds__(THREADS, 1)
+    umma_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmX,
+                          const __grid_constant__ CUtensorMap tmY, const Problem pr,
+                          const Epi epi) {
+  using L = SmemLayout<BN / 2, STAGES>;  // per CTA: 128 X rows + BN/2 Y rows per stage
+  static_assert(BN % 32 == 0 && BN >= 64 && BN <= 256, "pair MMA N in [64, 256]");
+  static_assert(2 * BN <= 512, "two accumulators must fit in TMEM");
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw = smem_u32(smem_raw);
+  const uint32_t base = (raw + 1023u) & ~1023u;
+  uint8_t *gbase = smem_raw + (base - raw);
+  const uint32_t bar0 = base + L::BAR_OFF;
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+  auto tfull_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };
+  auto tempty_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };
+  const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + L::BAR_OFF + L::BAR_BYTES);
+  volatile int *abort_flag = reinterpret_cast<volatile int *>(gbase + L::BAR_OFF + L::BAR_BYTES + 8);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  const int pair = (int)cluster_id_x(), npairs = (int)cluster_count_x();
+  const int total_tiles = pr.tiles_p * pr.tiles_q * pr.nbatch;
+  const uint32_t peer_abort = map_rank(smem_u32((const void *)abort_flag), rank ^ 1u);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(tfull_bar(a), 1);
+      mbar_init(tempty_bar(a), 8);  // 4 epilogue warps in each CTA of the pair
+    }
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    prefetch_tmap(&tmX);
+    prefetch_tmap(&tmY);
+  }
+  cluster_sync();  // both CTAs' barriers exist before any remote signal
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(2 * BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  cluster_sync();  // both CTAs hold the accumulator columns before the first MMA
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      const int kcoord = KBLOCK_BYTES / elem_bytes(KIND);
+      int stage = 0;
+      uint32_t phase = 0;
+      long issued = 0;
+      bool ok = true;
+      for (int t = pair; t < total_tiles && ok; t += npairs) {
+        int b, tp, tq;
+        tile_coords(pr, t, b, tp, tq);
+        const int xrow = tp * PAIR_BM + (int)rank * BM;
+        const int yrow = tq * BN + (int)rank * (BN / 2);
+        for (int kb = 0; kb < pr.kblocks; ++kb) {
+          if (!mbar_wait_pair(empty_bar(stage), phase ^ 1u, abort_flag, peer_abort, pr.derr)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sx = base + stage * L::STAGE_BYTES;
+          const uint32_t sy = sx + L::X_BYTES;
+          const uint32_t fb = map_rank(full_bar(stage), 0);
+          if (leader) mbar_expect_tx(full_bar(stage), 2 * L::STAGE_BYTES);
+          tma_load_3d_pair(sx, &tmX, fb, kb * kcoord, xrow, b);
+          tma_load_3d_pair(sy, &tmY, fb, kb * kcoord, yrow, b);
+          ++issued;
+          if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+        }
+      }
+      if (*abort_flag) {
+        if (leader) {
+          // Wait (bounded) until the fills this CTA posted have landed.
+          long first = issued - STAGES > 0 ? issued - STAGES : 0;
+          for (long i = first; i < issued; ++i) {
+            const int s = (int)(i % STAGES);
+            const uint32_t ph = (uint32_t)((i / STAGES) & 1);
+            const uint64_t t0 = gtimer();
+            while (!mbar_try_wait(full_bar(s), ph) && gtimer() - t0 < B2_WAIT_NS) {
+            }
+          }
+        } else {
+          // The odd CTA cannot observe the leader's barrier: give its last
+          // copies a millisecond (they take microseconds) before leaving.
+          const uint64_t t0 = gtimer();
+          while (gtimer() - t0 < 1000000ull) {
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------- MMA issuer (leader only)
+    if (leader && lane == 0) {
+      constexpr uint32_t idesc = make_idesc(KIND, PAIR_BM, BN);
+      int stage = 0;
+      uint32_t phase = 0;
+      int it = 0;
+      bool ok = true;
+      for (int t = pair; t < total_tiles && ok; t += npairs, ++it) {
+        const int acc = it & 1;
+        const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+        if (!mbar_wait_pair(tempty_bar(acc), acc_phase ^ 1u, abort_flag, peer_abort, pr.derr)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+        for (int kb = 0; kb < pr.kblocks; ++kb) {
+          if (!mbar_wait_pair(full_bar(stage), phase, abort_flag, peer_abort, pr.derr)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t sx = base + stage * L::STAGE_BYTES;
+          const uint32_t sy = sx + L::X_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < KBLOCK_BYTES / 32; ++kk) {
+            tc_mma_pair<KIND>(d_tmem, sw128_desc(sx + kk * 32), sw128_desc(sy + kk * 32), idesc,
+                              (kb | kk) ? 1u : 0u);
+          }
+          tc_commit_pair(empty_bar(stage), (uint16_t)3);  // frees the stage in both CTAs
+          if (++stage == STAGES) { stage = 0; phase ^= 1u; }
+        }
+        if (!ok) break;
+        tc_commit_pair(tfull_bar(acc), (uint16_t)3);
+      }
+      tc_commit_pair(drain_bar, (uint16_t)1);
+      const uint64_t t0 = gtimer();
+      while (!mbar_try_wait(drain_bar, 0) && gtimer() - t0 < B2_WAIT_NS) {
+      }
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue
+    const int quarter = warp & 3;
+    int it = 0;
+    for (int t = pair; t < total_tiles; t += npairs, ++it) {
+      int b, tp, tq;
+      tile_coords(pr, t, b, tp, tq);
+      const int acc = it & 1;
+      const bool ok = mbar_wait_pair(tfull_bar(acc), (uint32_t)((it >> 1) & 1), abort_flag,
+                                     peer_abort, pr.derr);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+      const int p = tp * PAIR_BM + (int)rank * BM + quarter * 32 + lane;
+      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
+#pragma unroll 1
+      for (int c = 0; c < BN / 32; ++c) {
+        uint32_t v[32];
+        tmem_ld32(taddr + (uint32_t)(c * 32), v);
+        tmem_ld_wait(v);
+        epi(b, p, tq * BN + c * 32, v);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(map_rank(tempty_bar(acc), 0));
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync();
+  tc_fence_after();
+  if (warp == 1) {
+    __syncwarp();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                 "r"(2 * BN));
+  }
+}
+
 // ------------------------------------------------------------------ host --
 // 3-D tensor map over `nbatch` planes of `rows` x `kelems` K-major elements
 // (row pitch `row_bytes`, plane pitch `plane_bytes`, both multiples of 16),
@@ -414,6 +705,65 @@ int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long lo
   B2_PROF(prof_name, s);
   kern<<<grid, THREADS, L::TOTAL, s>>>(tmX, tmY, pr, epi);
   e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, prof_name);
+  return B2_OK;
+}
+
+// Pair launch: clusters of 2 CTAs, one pair per two SMs (as many pairs as can
+// be resident at once, queried once per device), tiles of 256 X rows x BN Y
+// rows.  tmX must have a 128-row box and tmY a BN/2-row box.
+template <int KIND, int BN, int STAGES, class Epi>
+int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
+                int nbatch, const Epi &epi, int device, int *derr, cudaStream_t s,
+                const char *prof_name) {
+  using L = SmemLayout<BN / 2, STAGES>;
+  Problem pr;
+  pr.P = P;
+  pr.Q = Q;
+  pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
+  pr.nbatch = nbatch;
+  pr.tiles_p = (P + PAIR_BM - 1) / PAIR_BM;
+  pr.tiles_q = (Q + BN - 1) / BN;
+  pr.group = 8;
+  pr.derr = derr;
+  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch;
+  if (total <= 0) return B2_OK;
+  auto kern = umma_gemm_pair_kernel<KIND, BN, STAGES, Epi>;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = L::TOTAL;
+  cfg.stream = s;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  static int resident_pairs[64] = {0};  // per device, filled on first use
+  const int dslot = device >= 0 && device < 64 ? device : 0;
+  if (resident_pairs[dslot] == 0) {
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
+    if (e != cudaSuccess) return cuda_fail(e, "umma pair smem attribute");
+    cfg.gridDim = dim3(2);
+    int nc = 0;
+    e = cudaOccupancyMaxActiveClusters(&nc, kern, &cfg);
+    if (e != cudaSuccess || nc < 1) {
+      (void)cudaGetLastError();
+      return e != cudaSuccess ? cuda_fail(e, "umma pair occupancy") : (int)B2_ERR_UNSUPPORTED;
+    }
+    resident_pairs[dslot] = nc;
+  } else {
+    cudaError_t e =
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
+    if (e != cudaSuccess) return cuda_fail(e, "umma pair smem attribute");
+  }
+  const int pairs = (int)(total < resident_pairs[dslot] ? total : resident_pairs[dslot]);
+  cfg.gridDim = dim3(2 * pairs);
+  B2_PROF(prof_name, s);
+  cudaError_t e = cudaLaunchKernelEx(&cfg, kern, tmX, tmY, pr, epi);
+  if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, prof_name);
   return B2_OK;
 }
