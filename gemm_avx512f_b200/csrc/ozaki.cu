@@ -53,27 +53,51 @@ struct CrtTable {
   int H;                 // scaling target: 2-norms scaled to <= 2^H
   long long W[OZ_MAX][3];  // CRT weights, 42-bit limbs (low first)
   long long Pl[3];       // P in 42-bit limbs
-  double Wd[OZ_MAX][4];  // CRT weights in 32-bit limbs
-  double Pd[4];          // P in 32-bit limbs
+  double Wd[OZ_MAX][4];  // CRT weights in reconstruction limbs (limb_of)
+  double Pd[4];          // P in reconstruction limbs
   double invP;
   double log2P;
 };
 
-__constant__ int c_mod[OZ_MAX];
-__constant__ float c_invf[OZ_MAX];
-__constant__ double c_invd[OZ_MAX];
-__constant__ unsigned c_k16[OZ_MAX];  // 2^16 mod m
-__constant__ unsigned c_k32[OZ_MAX];  // 2^32 mod m
-__constant__ unsigned c_k48[OZ_MAX];  // 2^48 mod m
-__constant__ unsigned c_off[OZ_MAX];  // m - (2^62 mod m): undoes the +2^62 offset
-__constant__ unsigned c_magic[OZ_MAX];  // floor(2^32 / m) + 1 (Barrett)
+// Modulus i as a compile-time function, so fully unrolled loops over the
+// moduli fold every derived constant into an immediate.
+__host__ __device__ constexpr unsigned mod_at(int i) {
+  return i == 0 ? 256u : i == 1 ? 255u : i == 2 ? 253u : i == 3 ? 251u : i == 4 ? 247u
+       : i == 5 ? 241u : i == 6 ? 239u : i == 7 ? 233u : i == 8 ? 229u : i == 9 ? 227u
+       : i == 10 ? 223u : i == 11 ? 217u : i == 12 ? 211u : i == 13 ? 199u : i == 14 ? 197u
+       : 193u;
+}
+constexpr bool moduli_agree() {
+  for (int i = 0; i < OZ_MAX; ++i)
+    if (mod_at(i) != (unsigned)kModuli[i]) return false;
+  return true;
+}
+static_assert(moduli_agree(), "mod_at must list kModuli in order");
+
+// Epilogue constants, indexed by the batch (= modulus) of a GEMM tile:
+// m, bias = m * ceil(2^30 / m) (makes any |d| <= 2^30 non-negative without
+// changing d mod m) and the exact Barrett multiplier ceil(2^39 / m).
+__constant__ unsigned c_mod[OZ_MAX];
+__constant__ unsigned c_ebias[OZ_MAX];
+__constant__ unsigned c_m39[OZ_MAX];
 // CRT tables for every modulus count s = 0..OZ_MAX (index s), uploaded once per
 // device so calls with different counts never re-upload or synchronise.
-__constant__ double c_Wd[OZ_MAX + 1][OZ_MAX][4];  // weights in 32-bit limbs (low first)
-__constant__ double c_Pd[OZ_MAX + 1][4];          // P in 32-bit limbs
+__constant__ double c_Wd[OZ_MAX + 1][OZ_MAX][4];  // weights in limb_of limbs (low first)
+__constant__ double c_Pd[OZ_MAX + 1][4];          // P in limb_of limbs
 __constant__ double c_invP[OZ_MAX + 1];
 
 typedef unsigned __int128 u128;
+
+// Limb l of x for the reconstruction with s moduli: 40-bit limbs (the third
+// holding everything above bit 80) when s <= 15, 32-bit limbs otherwise.
+double limb_of(u128 x, int l, int s) {
+  if (s <= 15) {
+    if (l >= 3) return 0.0;
+    const u128 v = l == 2 ? (x >> 80) : ((x >> (40 * l)) & (((u128)1 << 40) - 1));
+    return (double)(unsigned long long)v;
+  }
+  return (double)(unsigned long long)((x >> (32 * l)) & 0xFFFFFFFFu);
+}
 
 CrtTable make_table(int s) {
   CrtTable t{};
@@ -97,9 +121,10 @@ CrtTable make_table(int s) {
     t.W[i][0] = (long long)(W & (u128)(LIMB - 1));
     t.W[i][1] = (long long)((W >> 42) & (u128)(LIMB - 1));
     t.W[i][2] = (long long)(W >> 84);
-    for (int l = 0; l < 4; ++l) t.Wd[i][l] = (double)(unsigned long long)((W >> (32 * l)) & 0xFFFFFFFFu);
+    // limbs of the reconstruction: 3 x 40 bits for s <= 15 (P < 2^118), else 4 x 32
+    for (int l = 0; l < 4; ++l) t.Wd[i][l] = limb_of(W, l, s);
   }
-  for (int l = 0; l < 4; ++l) t.Pd[l] = (double)(unsigned long long)((P >> (32 * l)) & 0xFFFFFFFFu);
+  for (int l = 0; l < 4; ++l) t.Pd[l] = limb_of(P, l, s);
   t.Pl[0] = (long long)(P & (u128)(LIMB - 1));
   t.Pl[1] = (long long)((P >> 42) & (u128)(LIMB - 1));
   t.Pl[2] = (long long)(P >> 84);
@@ -114,58 +139,112 @@ CrtTable make_table(int s) {
 // than K 2^-1022, negligible against max^2 >= 2^-960.  Rows outside that
 // range, and rows holding Inf/NaN (their sum turns non-finite), are redone
 // by the finalize kernel with a power-of-two-scaled sum.
-template <bool ROWCONT>
-__global__ void norm_partial_kernel(const double *__restrict__ X, long long sr, long long sk,
-                                    int R, int K, int kchunk, double *__restrict__ pmax,
-                                    double *__restrict__ pssq) {
+// Rows contiguous (element (r,k) at X[r + k*sk]): each thread owns 4
+// consecutive rows (two 16-byte loads per column when X and sk allow), a
+// 256-thread block covers 1024 rows, so every column of a block is one 8 KB
+// contiguous read, with 4 columns (128 B per thread) in flight.
+__global__ void __launch_bounds__(256)
+    norm_partial_rows_kernel(const double *__restrict__ X, long long sk, int R, int K, int kchunk,
+                             bool vec, double *__restrict__ pmax, double *__restrict__ pssq) {
   const int chunk = blockIdx.y;
   const int k0 = chunk * kchunk, k1 = min(K, k0 + kchunk);
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
-  int r;
-  if (ROWCONT) {
-    r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= R) return;
-    const double *p = X + r;
+  const int r0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (r0 >= R) return;
+  double sa[4] = {0.0, 0.0, 0.0, 0.0}, ma[4] = {0.0, 0.0, 0.0, 0.0};
+  const double *p = X + r0;
+  if (vec && r0 + 3 < R) {
     int k = k0;
     for (; k + 3 < k1; k += 4) {
-      const double a0 = __ldg(p + (long long)k * sk), a1 = __ldg(p + (long long)(k + 1) * sk);
-      const double a2 = __ldg(p + (long long)(k + 2) * sk), a3 = __ldg(p + (long long)(k + 3) * sk);
-      s0 = fma(a0, a0, s0); s1 = fma(a1, a1, s1); s2 = fma(a2, a2, s2); s3 = fma(a3, a3, s3);
-      m0 = fmax(m0, fabs(a0)); m1 = fmax(m1, fabs(a1)); m2 = fmax(m2, fabs(a2)); m3 = fmax(m3, fabs(a3));
+      double2 a[4][2];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double2 *q = reinterpret_cast<const double2 *>(p + (long long)(k + j) * sk);
+        a[j][0] = __ldg(q);
+        a[j][1] = __ldg(q + 1);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double v[4] = {a[j][0].x, a[j][0].y, a[j][1].x, a[j][1].y};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) { sa[e] = fma(v[e], v[e], sa[e]); ma[e] = fmax(ma[e], fabs(v[e])); }
+      }
     }
     for (; k < k1; ++k) {
-      const double a0 = __ldg(p + (long long)k * sk);
-      s0 = fma(a0, a0, s0);
-      m0 = fmax(m0, fabs(a0));
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const double v = __ldg(p + (long long)k * sk + e);
+        sa[e] = fma(v, v, sa[e]);
+        ma[e] = fmax(ma[e], fabs(v));
+      }
     }
   } else {
-    const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
-    r = blockIdx.x * warps + (threadIdx.x >> 5);
-    if (r >= R) return;
-    const double *p = X + (long long)r * sr;
-    int k = k0 + lane;
-    for (; k + 96 < k1; k += 128) {
-      const double a0 = __ldg(p + k), a1 = __ldg(p + k + 32), a2 = __ldg(p + k + 64),
-                   a3 = __ldg(p + k + 96);
-      s0 = fma(a0, a0, s0); s1 = fma(a1, a1, s1); s2 = fma(a2, a2, s2); s3 = fma(a3, a3, s3);
-      m0 = fmax(m0, fabs(a0)); m1 = fmax(m1, fabs(a1)); m2 = fmax(m2, fabs(a2)); m3 = fmax(m3, fabs(a3));
+    for (int e = 0; e < 4 && r0 + e < R; ++e)
+      for (int k = k0; k < k1; ++k) {
+        const double v = __ldg(p + (long long)k * sk + e);
+        sa[e] = fma(v, v, sa[e]);
+        ma[e] = fmax(ma[e], fabs(v));
+      }
+  }
+  for (int e = 0; e < 4 && r0 + e < R; ++e) {
+    pmax[(long long)chunk * R + r0 + e] = ma[e];
+    pssq[(long long)chunk * R + r0 + e] = sa[e];
+  }
+}
+
+// K contiguous (element (r,k) at X[r*sr + k]): one warp per row; lanes read
+// 16-byte pairs (when X, sr and the chunk start allow), 4 pairs in flight.
+__global__ void __launch_bounds__(256)
+    norm_partial_kcont_kernel(const double *__restrict__ X, long long sr, int R, int K,
+                              int kchunk, bool vec, double *__restrict__ pmax,
+                              double *__restrict__ pssq) {
+  const int chunk = blockIdx.y;
+  const int k0 = chunk * kchunk, k1 = min(K, k0 + kchunk);
+  const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.x * warps + (threadIdx.x >> 5);
+  if (r >= R) return;
+  const double *p = X + (long long)r * sr;
+  double sa[4] = {0.0, 0.0, 0.0, 0.0}, ma[4] = {0.0, 0.0, 0.0, 0.0};
+  if (vec && (k0 & 1) == 0) {
+    int k = k0 + 2 * lane;
+    for (; k + 193 < k1; k += 256) {
+      double2 a[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) a[j] = __ldg(reinterpret_cast<const double2 *>(p + k + 64 * j));
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        sa[j] = fma(a[j].x, a[j].x, sa[j]);
+        sa[j] = fma(a[j].y, a[j].y, sa[j]);
+        ma[j] = fmax(ma[j], fmax(fabs(a[j].x), fabs(a[j].y)));
+      }
     }
-    for (; k < k1; k += 32) {
-      const double a0 = __ldg(p + k);
-      s0 = fma(a0, a0, s0);
-      m0 = fmax(m0, fabs(a0));
+    for (; k + 1 < k1; k += 64) {
+      const double2 a = __ldg(reinterpret_cast<const double2 *>(p + k));
+      sa[0] = fma(a.x, a.x, sa[0]);
+      sa[0] = fma(a.y, a.y, sa[0]);
+      ma[0] = fmax(ma[0], fmax(fabs(a.x), fabs(a.y)));
+    }
+    if (k < k1) {
+      const double v = __ldg(p + k);
+      sa[0] = fma(v, v, sa[0]);
+      ma[0] = fmax(ma[0], fabs(v));
+    }
+  } else {
+    for (int k = k0 + lane; k < k1; k += 32) {
+      const double v = __ldg(p + k);
+      sa[0] = fma(v, v, sa[0]);
+      ma[0] = fmax(ma[0], fabs(v));
     }
   }
-  double s = (s0 + s1) + (s2 + s3), mx = fmax(fmax(m0, m1), fmax(m2, m3));
-  if (!ROWCONT) {
-    for (int o = 16; o > 0; o >>= 1) {
-      s += __shfl_down_sync(0xffffffffu, s, o);
-      mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    }
-    if ((threadIdx.x & 31) != 0) return;
+  double s = (sa[0] + sa[1]) + (sa[2] + sa[3]);
+  double mx = fmax(fmax(ma[0], ma[1]), fmax(ma[2], ma[3]));
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
   }
-  pmax[(long long)chunk * R + r] = mx;
-  pssq[(long long)chunk * R + r] = s;
+  if (lane == 0) {
+    pmax[(long long)chunk * R + r] = mx;
+    pssq[(long long)chunk * R + r] = s;
+  }
 }
 
 // Scaled sum of squares for the rare rows outside the fast range:
@@ -217,20 +296,61 @@ __global__ void norm_finalize_kernel(const double *__restrict__ pmax,
 }
 
 // --------------------------------------------------------- residue slices --
-// x + 2^62 >= 0 is split into 16-bit limbs c3..c0 (c3 < 2^15); the limb sum
-// with the precomputed powers 2^16j mod m, plus (m - 2^62 mod m) to undo the
-// offset, stays below 2^26 + 256.  Barrett with magic = floor(2^32/m) + 1
-// over-estimates the quotient by at most s/2^32 < 1/64, so one correction
-// brings s - q m into [0, m); the symmetric representative follows.
-__device__ __forceinline__ int sym_residue(unsigned c0, unsigned c1, unsigned c2, unsigned c3,
-                                           int i) {
-  const int m = c_mod[i];
-  const unsigned s = c0 + c1 * c_k16[i] + c2 * c_k32[i] + c3 * c_k48[i] + c_off[i];
-  const unsigned q = __umulhi(s, c_magic[i]);
-  int r = (int)(s - q * (unsigned)m);
-  r += (r < 0) ? m : 0;
-  r -= (r > ((m - 1) >> 1)) ? m : 0;
-  return r;
+// u = x + 2^62 in [0, 2^63) is split into 21-bit limbs c0, c1, c2 (< 2^21).
+// For modulus m with h = floor(m/2):
+//   sh = c0 + c1 (2^21 mod m) + c2 (2^42 mod m) + ((-2^62 mod m) + h)
+// is congruent to x + h, and sh <= (2^21 - 1) 511 + 383 < 2^30.  Then
+// q = floor(sh * ceil(2^38/m) / 2^38) is exactly floor(sh/m): with
+// ceil(2^38/m) = 2^38/m + d, 0 <= d < 1, the excess sh d / 2^38 < 2^-8 <= 1/m
+// cannot carry the fraction of sh/m past the next integer.  sh - q m lies in
+// [0, m), so sh - q m - h is the symmetric residue of x, in [-h, m-1-h]
+// (int8 for every modulus <= 256).  Six integer operations per modulus.
+struct SliceConst {
+  unsigned m, h, k21, k42, offh, m38;
+};
+__host__ __device__ constexpr SliceConst slice_const(int i) {
+  return SliceConst{mod_at(i), mod_at(i) >> 1, (1u << 21) % mod_at(i),
+                    (unsigned)((1ull << 42) % mod_at(i)),
+                    (unsigned)((mod_at(i) - (1ull << 62) % mod_at(i)) % mod_at(i) + (mod_at(i) >> 1)),
+                    (unsigned)(((1ull << 38) + mod_at(i) - 1) / mod_at(i))};
+}
+
+// Two's-complement byte of the symmetric residue (in the low 8 bits).
+template <int I>
+__device__ __forceinline__ unsigned sym_residue_byte(unsigned c0, unsigned c1, unsigned c2) {
+  constexpr SliceConst K = slice_const(I);
+  const unsigned sh = c0 + c1 * K.k21 + c2 * K.k42 + K.offh;
+  const unsigned q = __umulhi(sh, K.m38) >> 6;
+  return sh - q * K.m - K.h;
+}
+
+// Writes the 8 residue bytes of one thread's elements for modulus I.
+template <int I>
+__device__ __forceinline__ void store_slice(const unsigned (&c0)[8], const unsigned (&c1)[8],
+                                            const unsigned (&c2)[8], int8_t *dst, int nk) {
+  unsigned r[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) r[j] = sym_residue_byte<I>(c0[j], c1[j], c2[j]);
+  const unsigned lo = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040),
+                                  0x5410);
+  const unsigned hi = __byte_perm(__byte_perm(r[4], r[5], 0x0040), __byte_perm(r[6], r[7], 0x0040),
+                                  0x5410);
+  if (nk == 8) {
+    *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+  } else {
+    for (int j = 0; j < nk; ++j) dst[j] = (int8_t)(r[j] & 0xFFu);
+  }
+}
+
+template <int I>
+__device__ __forceinline__ void store_slices(const unsigned (&c0)[8], const unsigned (&c1)[8],
+                                             const unsigned (&c2)[8], int s, int8_t *dst,
+                                             long long plane, int nk) {
+  if constexpr (I < OZ_MAX) {
+    if (I >= s) return;
+    store_slice<I>(c0, c1, c2, dst + (long long)I * plane, nk);
+    store_slices<I + 1>(c0, c1, c2, s, dst, plane, nk);
+  }
 }
 
 __device__ __forceinline__ double pow2(int e) {  // e in [-1022, 1023]
@@ -268,32 +388,17 @@ __global__ void __launch_bounds__(256)
   // 2^sigma as two in-range factors (sigma in [H-1024, H+1074])
   const int e1 = dead ? 0 : (sg > 1000 ? 1000 : (sg < -1000 ? -1000 : sg));
   const double f1 = pow2(e1), f2 = pow2(dead ? 0 : sg - e1);
-  unsigned c0[8], c1[8], c2[8], c3[8];
+  unsigned c0[8], c1[8], c2[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const double v = dead ? 0.0 : (tile[rr][kg + j] * f1) * f2;
     const unsigned long long u = (unsigned long long)(__double2ll_rz(v) + (1ll << 62));
-    c0[j] = (unsigned)(u & 0xFFFFull);
-    c1[j] = (unsigned)((u >> 16) & 0xFFFFull);
-    c2[j] = (unsigned)((u >> 32) & 0xFFFFull);
-    c3[j] = (unsigned)(u >> 48);
+    c0[j] = (unsigned)u & 0x1FFFFFu;
+    c1[j] = (unsigned)(u >> 21) & 0x1FFFFFu;
+    c2[j] = (unsigned)(u >> 42);
   }
   const int nk = min(8, K - (k0 + kg));
-  for (int i = 0; i < s; ++i) {
-    unsigned lo = 0, hi = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const unsigned b = (unsigned)(sym_residue(c0[j], c1[j], c2[j], c3[j], i) & 0xFF);
-      if (j < 4) lo |= b << (8 * j); else hi |= b << (8 * (j - 4));
-    }
-    int8_t *dst = out + (long long)i * plane + (long long)r * kp + k0 + kg;
-    if (nk == 8) {
-      *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
-    } else {
-      for (int j = 0; j < nk; ++j)
-        dst[j] = (int8_t)((j < 4 ? lo >> (8 * j) : hi >> (8 * (j - 4))) & 0xFF);
-    }
-  }
+  store_slices<0>(c0, c1, c2, s, out + (long long)r * kp + k0 + kg, plane, nk);
 }
 
 // ---------------------------------------------------------- GEMM epilogue --
@@ -307,29 +412,29 @@ struct ResidueEpi {
   int accumulate;  // add onto the stored residue (K chunks after the first)
   __device__ __forceinline__ void operator()(int b, int p, int q0, const uint32_t (&v)[32]) const {
     if (p >= P || q0 >= Q) return;
-    const int m = c_mod[b];
-    const double inv = c_invd[b];
+    // d mod m for |d| <= 2^30 (K <= 65536 products of |r| <= 128): e = d + bias
+    // lies in [0, 2^31 + 256), and floor(e * ceil(2^39/m) / 2^39) is exactly
+    // floor(e/m) because the excess e d' / 2^39 (d' < 1) stays below
+    // 1/256 + 2^-31 < 1/m for m <= 255 (and is 0 for m = 256).
+    const unsigned m = c_mod[b], bias = c_ebias[b], m39 = c_m39[b];
     uint8_t *dst = R + (long long)b * plane + (long long)p * ldr + q0;
     uint32_t w[8];
 #pragma unroll
     for (int g = 0; g < 8; ++g) {
-      uint32_t word = 0;
+      unsigned r4[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const int d = (int)v[4 * g + j];
-        int q = __double2int_rd((double)d * inv);
-        int r = d - q * m;
-        r += (r < 0) ? m : 0;
-        r -= (r >= m) ? m : 0;
-        word |= (uint32_t)r << (8 * j);
+        const unsigned e = v[4 * g + j] + bias;
+        r4[j] = e - (__umulhi(e, m39) >> 7) * m;
       }
-      w[g] = word;
+      w[g] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040), __byte_perm(r4[2], r4[3], 0x0040),
+                         0x5410);
     }
     const int nq = min(32, Q - q0);
     if (accumulate) {
       for (int j = 0; j < nq; ++j) {
-        int r = (int)((w[j >> 2] >> (8 * (j & 3))) & 0xFF) + (int)dst[j];
-        r -= (r >= m) ? m : 0;
+        unsigned r = ((w[j >> 2] >> (8 * (j & 3))) & 0xFFu) + (unsigned)dst[j];
+        r -= (r >= m) ? m : 0u;
         dst[j] = (uint8_t)r;
       }
     } else if (nq == 32) {
@@ -357,42 +462,72 @@ __device__ __forceinline__ double byte_to_double(unsigned b) {  // exact, no con
 
 // C(m,n) = alpha * C'(m,n) 2^-(sigma_m + tau_n) + beta C(m,n).  C' is the value
 // in (-P/2, P/2) with the s residues: S = sum_i r_i W_i is accumulated exactly
-// in four 32-bit limbs held in doubles (r_i W_il < 2^40, sums < 2^44), the
-// quotient q = round(S/P) comes from one double estimate (|C'| <= P/4 keeps it
-// exact), S - qP is exact per limb, and the carries are settled in 64-bit
-// integers.  Each thread handles 4 consecutive rows m of one column n.
+// in limbs held in doubles -- three 40-bit limbs when s <= 15 (r_i W_il <
+// 2^48, sums < 15 * 2^48 < 2^52), four 32-bit limbs for s = 16 -- the quotient
+// q = round(S/P) comes from one double estimate (|C'| <= P/4 keeps it exact),
+// S - qP is exact per limb (q P_l < 2^52), and the carries are settled in
+// 64-bit integers.  Each thread handles 4 consecutive rows m of one column n.
 // Rows/columns flagged NONFINITE use a direct FP64 dot product.
+template <int LIMBS>
 __global__ void __launch_bounds__(256)
     reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr, int s, int M,
                        int N, const int *__restrict__ sigA, const int *__restrict__ tauB,
                        double alpha, double beta, double *__restrict__ C, int ldc,
                        const double *__restrict__ A, long long asr, long long ask,
                        const double *__restrict__ B, long long bsk, long long bsc, int K) {
-  const int M4 = (M + 3) >> 2;
-  const long long total = (long long)M4 * N;
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const int m0 = (int)(idx % M4) * 4, n = (int)(idx / M4);
-    double S[4][4];
+  static_assert(LIMBS == 3 || LIMBS == 4, "3 x 40-bit or 4 x 32-bit limbs");
+  constexpr int LB = LIMBS == 3 ? 40 : 32;
+  // Grid: x covers the rows m in groups of 4 per thread, y strides over the
+  // columns n (no integer division per item).
+  const int m0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  if (m0 >= M) return;
+  // C as two 16-byte pairs per thread when every 4-row group is 16-byte aligned
+  const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && ((ldc & 1) == 0);
+  const bool full = vec && m0 + 3 < M;
+  for (int n = blockIdx.y; n < N; n += gridDim.y) {
+    // Issue every load of this item first (s residue words, 4 C values): the
+    // pass is bound by memory latency unless they are all in flight together.
+    const uint8_t *rp = R + (long long)n * ldr + m0;
+    unsigned w[OZ_MAX];
+#pragma unroll
+    for (int i = 0; i < OZ_MAX; ++i)
+      w[i] = i < s ? __ldg(reinterpret_cast<const unsigned *>(rp + (long long)i * plane)) : 0u;
+    double *cp = C + (long long)n * ldc + m0;
+    double cold[4];
+    if (full) {
+      const double2 c01 = *reinterpret_cast<const double2 *>(cp);
+      const double2 c23 = *reinterpret_cast<const double2 *>(cp + 2);
+      cold[0] = c01.x; cold[1] = c01.y; cold[2] = c23.x; cold[3] = c23.y;
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) cold[e] = m0 + e < M ? cp[e] : 0.0;
+    }
+    double S[4][LIMBS];
 #pragma unroll
     for (int e = 0; e < 4; ++e)
 #pragma unroll
-      for (int l = 0; l < 4; ++l) S[e][l] = 0.0;
-    const uint8_t *rp = R + (long long)n * ldr + m0;
-    for (int i = 0; i < s; ++i) {
-      const unsigned w4 = *reinterpret_cast<const unsigned *>(rp + (long long)i * plane);
+      for (int l = 0; l < LIMBS; ++l) S[e][l] = 0.0;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const double rd = byte_to_double((w4 >> (8 * e)) & 0xFFu);
+    for (int i = 0; i < OZ_MAX; ++i) {
+      if (i < s) {
+        double W[LIMBS];
 #pragma unroll
-        for (int l = 0; l < 4; ++l) S[e][l] = fma(rd, c_Wd[s][i][l], S[e][l]);
+        for (int l = 0; l < LIMBS; ++l) W[l] = c_Wd[s][i][l];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const double rd = byte_to_double((w[i] >> (8 * e)) & 0xFFu);
+#pragma unroll
+          for (int l = 0; l < LIMBS; ++l) S[e][l] = fma(rd, W[l], S[e][l]);
+        }
       }
     }
     const int tg = tauB[n];
+    double out[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int m = m0 + e;
-      if (m >= M) break;
+      out[e] = 0.0;
+      if (m >= M) continue;
       const int sg = sigA[m];
       double val;
       if (sg == NONFINITE || tg == NONFINITE) {
@@ -400,30 +535,63 @@ __global__ void __launch_bounds__(256)
         for (int k = 0; k < K; ++k) acc = fma(A[m * asr + k * ask], B[k * bsk + n * bsc], acc);
         val = acc;
       } else {
-        const double Sd =
-            fma(S[e][3], 0x1p96, fma(S[e][2], 0x1p64, fma(S[e][1], 0x1p32, S[e][0])));
+        double Sd = S[e][LIMBS - 1];
+#pragma unroll
+        for (int l = LIMBS - 2; l >= 0; --l) Sd = fma(Sd, (double)(1ull << LB), S[e][l]);
         const double q = rint(Sd * c_invP[s]);
-        long long X0 = __double2ll_rn(fma(-q, c_Pd[s][0], S[e][0]));
-        long long X1 = __double2ll_rn(fma(-q, c_Pd[s][1], S[e][1]));
-        long long X2 = __double2ll_rn(fma(-q, c_Pd[s][2], S[e][2]));
-        long long X3 = __double2ll_rn(fma(-q, c_Pd[s][3], S[e][3]));
-        long long cy = X0 >> 32;
-        X0 -= cy << 32;
-        X1 += cy;
-        cy = X1 >> 32;
-        X1 -= cy << 32;
-        X2 += cy;
-        cy = X2 >> 32;
-        X2 -= cy << 32;
-        X3 += cy;
-        const unsigned long long lo = ((unsigned long long)X1 << 32) | (unsigned long long)X0;
-        const long long hi = X3 * 4294967296ll + X2;
-        val = scalbn(i128_to_double(hi, lo), -(sg + tg));
+        long long X[LIMBS];
+#pragma unroll
+        for (int l = 0; l < LIMBS; ++l) X[l] = __double2ll_rn(fma(-q, c_Pd[s][l], S[e][l]));
+#pragma unroll
+        for (int l = 0; l + 1 < LIMBS; ++l) {
+          const long long cy = X[l] >> LB;
+          X[l] -= cy * (1ll << LB);
+          X[l + 1] += cy;
+        }
+        unsigned long long lo;
+        long long hi;
+        if constexpr (LIMBS == 3) {  // X0 + X1 2^40 + X2 2^80, X0, X1 in [0, 2^40)
+          lo = (unsigned long long)X[0] | ((unsigned long long)X[1] << 40);
+          hi = (X[1] >> 24) + X[2] * 65536ll;
+        } else {  // X0 + X1 2^32 + X2 2^64 + X3 2^96, X0..X2 in [0, 2^32)
+          lo = ((unsigned long long)X[1] << 32) | (unsigned long long)X[0];
+          hi = X[3] * 4294967296ll + X[2];
+        }
+        // times 2^-(sg + tg) as two exact power-of-two factors: the first
+        // keeps the value normal, so the product rounds once
+        // (|C'| < 2^118: a remaining factor below 2^-1022 leaves less than the
+        // smallest subnormal, one above 2^1023 overflows any nonzero C')
+        const int ex = -(sg + tg);
+        const int e1 = ex > 1000 ? 1000 : (ex < -1000 ? -1000 : ex);
+        const int e2 = ex - e1;
+        const double f2 = e2 < -1022 ? 0.0 : pow2(e2 > 1023 ? 1023 : e2);
+        val = (i128_to_double(hi, lo) * pow2(e1)) * f2;
       }
-      double *cp = C + (long long)n * ldc + m;
-      *cp = (beta == 1.0) ? fma(alpha, val, *cp) : fma(alpha, val, beta * *cp);
+      out[e] = (beta == 1.0) ? fma(alpha, val, cold[e]) : fma(alpha, val, beta * cold[e]);
+    }
+    if (full) {
+      *reinterpret_cast<double2 *>(cp) = make_double2(out[0], out[1]);
+      *reinterpret_cast<double2 *>(cp + 2) = make_double2(out[2], out[3]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (m0 + e < M) cp[e] = out[e];
     }
   }
+}
+
+// Launch of the reconstruction with the limb width the modulus count allows.
+void launch_reconstruct(const uint8_t *R, long long plane, int ldr, int s, int M, int N,
+                        const int *sigA, const int *tauB, double alpha, double beta, double *C,
+                        int ldc, const double *A, long long asr, long long ask, const double *B,
+                        long long bsk, long long bsc, int K, cudaStream_t st) {
+  const dim3 blocks((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)(N < 65535 ? N : 65535));
+  if (s <= 15)
+    reconstruct_kernel<3><<<blocks, 256, 0, st>>>(R, plane, ldr, s, M, N, sigA, tauB, alpha, beta,
+                                                   C, ldc, A, asr, ask, B, bsk, bsc, K);
+  else
+    reconstruct_kernel<4><<<blocks, 256, 0, st>>>(R, plane, ldr, s, M, N, sigA, tauB, alpha, beta,
+                                                   C, ldc, A, asr, ask, B, bsk, bsc, K);
 }
 
 struct OzPlan {
@@ -439,19 +607,12 @@ int upload_tables(int dev, cudaStream_t st) {
   if (dev < 0 || dev >= 64) return B2_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lk(g_table_mu);
   if (g_table_done[dev]) return B2_OK;
-  int mod[OZ_MAX];
-  float invf[OZ_MAX];
-  double invd[OZ_MAX];
-  unsigned k16[OZ_MAX], k32[OZ_MAX], k48[OZ_MAX], off[OZ_MAX], magic[OZ_MAX];
+  unsigned mod[OZ_MAX], ebias[OZ_MAX], m39[OZ_MAX];
   for (int i = 0; i < OZ_MAX; ++i) {
-    mod[i] = kModuli[i];
-    invf[i] = 1.0f / (float)kModuli[i];
-    invd[i] = 1.0 / (double)kModuli[i];
-    k16[i] = (unsigned)((1ull << 16) % (unsigned long long)kModuli[i]);
-    k32[i] = (unsigned)((1ull << 32) % (unsigned long long)kModuli[i]);
-    k48[i] = (unsigned)((1ull << 48) % (unsigned long long)kModuli[i]);
-    off[i] = (unsigned)(kModuli[i] - (int)((1ull << 62) % (unsigned long long)kModuli[i]));
-    magic[i] = (unsigned)((1ull << 32) / (unsigned long long)kModuli[i] + 1);
+    const unsigned long long m = (unsigned long long)kModuli[i];
+    mod[i] = (unsigned)m;
+    ebias[i] = (unsigned)(m * (((1ull << 30) + m - 1) / m));
+    m39[i] = (unsigned)(((1ull << 39) + m - 1) / m);
   }
   static double wd[OZ_MAX + 1][OZ_MAX][4], pd[OZ_MAX + 1][4], ip[OZ_MAX + 1];
   memset(wd, 0, sizeof(wd));
@@ -464,13 +625,8 @@ int upload_tables(int dev, cudaStream_t st) {
     ip[s] = t.invP;
   }
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_mod, mod, sizeof(mod), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invf, invf, sizeof(invf), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invd, invd, sizeof(invd), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k16, k16, sizeof(k16), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k32, k32, sizeof(k32), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_k48, k48, sizeof(k48), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_off, off, sizeof(off), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_magic, magic, sizeof(magic), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_ebias, ebias, sizeof(ebias), 0, cudaMemcpyHostToDevice, st));
+  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_m39, m39, sizeof(m39), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Wd, wd, sizeof(wd), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Pd, pd, sizeof(pd), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_invP, ip, sizeof(ip), 0, cudaMemcpyHostToDevice, st));
@@ -526,32 +682,50 @@ int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, in
 }
 
 // Exponents for the R "rows" of an operand (element (r,k) at X[r*sr + k*sk]).
-// K chunks of the norm pass: about one per 1024 of K, more when there are few
-// rows (so at least ~16k rows x chunks are in flight), never below 64 of K each.
-int norm_chunks(int R, int K) {
-  int c = (K + 1023) / 1024;
-  if (c > 16) c = 16;
-  const int want = (16384 + R - 1) / (R > 0 ? R : 1);
-  if (c < want) c = want;
-  if (c > 64) c = 64;
-  const int maxc = K / 64 > 1 ? K / 64 : 1;
-  return c < maxc ? c : maxc;
+// K chunks of the norm pass.  Rows contiguous: enough 1024-row blocks x
+// chunks for ~8 blocks per SM (at most 128 chunks, at least 32 columns each).
+// K contiguous: rows x chunks >= 16384 warps (at most 64 chunks, at least 256
+// of K each).  The chunk length is rounded up to a multiple of 8.
+int norm_chunks(int R, int K, bool rowcont) {
+  if (R < 1) R = 1;
+  int c;
+  if (rowcont) {
+    const int rb = (R + 1023) / 1024;
+    c = (1184 + rb - 1) / rb;
+    if (c > 128) c = 128;
+    const int maxc = K / 32 > 1 ? K / 32 : 1;
+    if (c > maxc) c = maxc;
+  } else {
+    c = (16384 + R - 1) / R;
+    if (c > 64) c = 64;
+    const int maxc = K / 256 > 1 ? K / 256 : 1;
+    if (c > maxc) c = maxc;
+  }
+  return c > 1 ? c : 1;
 }
 
 int norm_exponents(const double *X, long long sr, long long sk, int R, int K, int H, int *sigma,
                    void *scratch, cudaStream_t s) {
-  const int chunks = norm_chunks(R, K);
-  const int kchunk = (K + chunks - 1) / chunks;
+  const bool rowcont = sr == 1;
+  const int want = norm_chunks(R, K, rowcont);
+  const int kchunk = K > 0 ? (int)round_up((K + want - 1) / want, 8) : 8;
+  const int chunks = K > 0 ? (K + kchunk - 1) / kchunk : 1;
   double *pmax = (double *)round_up((uintptr_t)scratch, 16);
   double *pssq = pmax + (long long)chunks * R;
-  if (sr == 1) {
-    dim3 grid((R + 127) / 128, chunks);
-    B2_PROF("ozaki_norm", s);
-    norm_partial_kernel<true><<<grid, 128, 0, s>>>(X, sr, sk, R, K, kchunk, pmax, pssq);
+  if (rowcont) {
+    const bool vec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && ((sk & 1) == 0);
+    dim3 grid((R + 1023) / 1024, chunks);
+    B2_PROF("ozaki_norm_rowcont", s);
+    norm_partial_rows_kernel<<<grid, 256, 0, s>>>(X, sk, R, K, kchunk, vec, pmax, pssq);
   } else {
+    const bool vec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && ((sr & 1) == 0) && sk == 1;
     dim3 grid((R + 7) / 8, chunks);
-    B2_PROF("ozaki_norm", s);
-    norm_partial_kernel<false><<<grid, 256, 0, s>>>(X, sr, sk, R, K, kchunk, pmax, pssq);
+    B2_PROF("ozaki_norm_kcont", s);
+    if (sk == 1) {
+      norm_partial_kcont_kernel<<<grid, 256, 0, s>>>(X, sr, R, K, kchunk, vec, pmax, pssq);
+    } else {
+      return B2_ERR_ARG;  // every operand view has one unit stride
+    }
   }
   B2_CUDA_TRY(cudaGetLastError());
   {
@@ -564,8 +738,8 @@ int norm_exponents(const double *X, long long sr, long long sk, int R, int K, in
 }
 
 size_t norm_scratch_bytes(int R, int K) {
-  const int chunks = norm_chunks(R, K);
-  return (size_t)chunks * R * 16 + 64;
+  const int a = norm_chunks(R, K, true), b = norm_chunks(R, K, false);
+  return (size_t)(a > b ? a : b) * R * 16 + 64;
 }
 
 }  // namespace
@@ -634,7 +808,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
     const int kc0 = c * KCH, kcl = (k - kc0 < KCH) ? k - kc0 : KCH;
     {
       dim3 grid((kcl + 63) / 64, (m + 31) / 32);
-      B2_PROF("ozaki_slice", st);
+      B2_PROF(asr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
       if (asr == 1)
         slice_kernel<true><<<grid, 256, 0, st>>>(A + kc0 * ask, asr, ask, m, kcl, sigA, s, Y, kp, planeY);
       else
@@ -643,7 +817,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
     }
     {
       dim3 grid((kcl + 63) / 64, (n + 31) / 32);
-      B2_PROF("ozaki_slice", st);
+      B2_PROF(bsr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
       if (bsr == 1)
         slice_kernel<true><<<grid, 256, 0, st>>>(B + kc0 * bsk, bsr, bsk, n, kcl, tauB, s, X, kp, planeX);
       else
@@ -656,11 +830,9 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   }
   if (rc != B2_OK) return rc;
   {
-    const long long total = (long long)((m + 3) / 4) * n;
-    const int blocks = (int)((total + 255) / 256 > 16384 ? 16384 : (total + 255) / 256);
     B2_PROF("ozaki_reconstruct", st);
-    reconstruct_kernel<<<blocks, 256, 0, st>>>(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha,
-                                                beta, C, ldc, A, asr, ask, B, bsk, bsr, k);
+    launch_reconstruct(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha, beta, C, ldc, A, asr, ask,
+                       B, bsk, bsr, k, st);
     B2_CUDA_TRY(cudaGetLastError());
   }
   g_last_plan.s = s;
@@ -819,12 +991,8 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   rc = umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, k, s, epi, prop.multiProcessorCount,
                                             derr, st, "ozaki_i8_gemm");
   if (rc != B2_OK) return rc;
-  {
-    const long long total = (long long)((m + 3) / 4) * n;
-    const int blocks = (int)((total + 255) / 256 > 16384 ? 16384 : (total + 255) / 256);
-    reconstruct_kernel<<<blocks, 256, 0, st>>>(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha,
-                                                beta, C, ldc, A, asr, ask, B, bsk, bsr, k);
-    B2_CUDA_TRY(cudaGetLastError());
-  }
+  launch_reconstruct(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha, beta, C, ldc, A, asr, ask, B,
+                     bsk, bsr, k, st);
+  B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
