@@ -42,6 +42,12 @@ struct CtxOwner {
       if (c->ws[i]) cudaFree(c->ws[i]);
     if (c->derr) cudaFree(c->derr);
     if (c->pinned) cudaFreeHost(c->pinned);
+    if (c->h2d) cudaStreamSynchronize(c->h2d), cudaStreamDestroy(c->h2d);
+    if (c->d2h) cudaStreamSynchronize(c->d2h), cudaStreamDestroy(c->d2h);
+    for (int i = 0; i < Ctx::PIPE_MAX; ++i) {
+      if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
+      if (c->ev_done[i]) cudaEventDestroy(c->ev_done[i]);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
   }
@@ -78,10 +84,20 @@ Ctx *ctx() {
   c->cc_minor = prop.minor;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&c->derr, 64) != cudaSuccess || cudaMemset(c->derr, 0, 64) != cudaSuccess ||
-      cudaMallocHost(&c->pinned, 4096) != cudaSuccess) {
+      cudaMallocHost(&c->pinned, 4096) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking) != cudaSuccess) {
     (void)cudaGetLastError();
     delete c;
     return nullptr;
+  }
+  for (int i = 0; i < Ctx::PIPE_MAX; ++i) {
+    if (cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming) != cudaSuccess) {
+      (void)cudaGetLastError();
+      delete c;
+      return nullptr;
+    }
   }
   c->dgemm_method = method_from_env(getenv("B2_METHOD"), B2_METHOD_FP64);
   c->sgemm_method = method_from_env(getenv("B2_SGEMM_METHOD"), B2_METHOD_FP32);
@@ -141,7 +157,7 @@ int stage_in(Ctx *c, int slot, const void *host, int rows, int cols, int ld, siz
   if (!d) return B2_ERR_NOMEM;
   if (rows > 0 && cols > 0)
     B2_CUDA_TRY(cudaMemcpy2DAsync(d, (size_t)ldd * elem, host, (size_t)ld * elem, (size_t)rows * elem,
-                                  cols, cudaMemcpyHostToDevice, s));
+                                  cols, cudaMemcpyDefault, s));
   *dev = d;
   *dld = ldd > 0 ? ldd : 2;
   return B2_OK;
@@ -151,7 +167,7 @@ int stage_out(void *host, int ld, const void *dev, int dld, int rows, int cols, 
               cudaStream_t s) {
   if (rows > 0 && cols > 0)
     B2_CUDA_TRY(cudaMemcpy2DAsync(host, (size_t)ld * elem, dev, (size_t)dld * elem, (size_t)rows * elem,
-                                  cols, cudaMemcpyDeviceToHost, s));
+                                  cols, cudaMemcpyDefault, s));
   return B2_OK;
 }
 
@@ -198,7 +214,31 @@ int sgemm_device(char ta, char tb, int m, int n, int k, float alpha, const float
   return sgemm_dispatch(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method, s);
 }
 
-// Shared host-or-device driver for the real drop-in GEMMs.
+// Column blocks of the host-operand pipeline: blocks of a multiple of 256
+// columns moving about 128 MB each (A, B and C counted), 2..PIPE_MAX blocks;
+// 1 (no pipeline) for products under 2^32 flops.
+static int pipeline_blocks(int m, int n, int k, size_t elem, int *cols) {
+  const double flops = 2.0 * m * (double)n * k;
+  *cols = n;
+  if (flops < 4294967296.0 || n < 512) return 1;
+  const double per_col = (double)(m + k) * elem;
+  int cw = (int)(134217728.0 / per_col);
+  cw = (cw + 255) / 256 * 256;
+  if (cw < 256) cw = 256;
+  int nb = (n + cw - 1) / cw;
+  if (nb < 2) { cw = ((n + 1) / 2 + 255) / 256 * 256; nb = (n + cw - 1) / cw; }
+  if (nb > Ctx::PIPE_MAX) { cw = ((n + Ctx::PIPE_MAX - 1) / Ctx::PIPE_MAX + 255) / 256 * 256; nb = (n + cw - 1) / cw; }
+  *cols = cw;
+  return nb;
+}
+
+// Shared host-or-device driver for the real drop-in GEMMs.  run(A, lda, B,
+// ldb, C, ldc, ncols, stream) computes columns [0, ncols) of C from the B
+// columns it is given.  Host operands of a large product go through a
+// three-stream pipeline over column blocks of B and C: A is copied once, then
+// block j is copied in (copy-in stream), computed (library stream) and copied
+// out (copy-out stream) while block j+1 is copied in, so the PCIe transfers,
+// which dominate a host-to-host product, overlap the GEMM.
 template <typename T, typename F>
 static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *a, int lda,
                        const T *b, int ldb, T beta, T *cm, int ldc, F &&run) {
@@ -212,20 +252,75 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
   const bool need_ab = (k > 0 && alpha != (T)0);
   const bool dev = is_device_ptr(cm) && (!need_ab || (is_device_ptr(a) && is_device_ptr(b)));
   if (dev) {
-    st = run(a, lda, b, ldb, cm, ldc, s);
+    st = run(a, lda, b, ldb, cm, ldc, n, s);
   } else {
     const int ra = notrans(ta) ? m : k, ca = notrans(ta) ? k : m;
     const int rb = notrans(tb) ? k : n, cb = notrans(tb) ? n : k;
     void *da = nullptr, *db = nullptr, *dc = nullptr;
     int dla = 2, dlb = 2, dlc = 2;
+    int cw = n;
+    const int nb = need_ab ? pipeline_blocks(m, n, k, sizeof(T), &cw) : 1;
     st = B2_OK;
-    if (need_ab) {
-      st = stage_in(c, WS_STAGE_A, a, ra, ca, lda, sizeof(T), &da, &dla, s);
-      if (st == B2_OK) st = stage_in(c, WS_STAGE_B, b, rb, cb, ldb, sizeof(T), &db, &dlb, s);
+    if (nb == 1) {
+      if (need_ab) {
+        st = stage_in(c, WS_STAGE_A, a, ra, ca, lda, sizeof(T), &da, &dla, s);
+        if (st == B2_OK) st = stage_in(c, WS_STAGE_B, b, rb, cb, ldb, sizeof(T), &db, &dlb, s);
+      }
+      if (st == B2_OK) st = stage_in(c, WS_STAGE_C, cm, m, n, ldc, sizeof(T), &dc, &dlc, s);
+      if (st == B2_OK) st = run((const T *)da, dla, (const T *)db, dlb, (T *)dc, dlc, n, s);
+      if (st == B2_OK) st = stage_out(cm, ldc, dc, dlc, m, n, sizeof(T), s);
+    } else {
+      // Full-size device copies (no buffer is reused, so no block waits for
+      // another's copy-out); the column block j of op(B) is B's columns
+      // [j0, j1) for 'N' and its rows [j0, j1) for 'T'.
+      dla = (ra + 1) & ~1;
+      dlb = (rb + 1) & ~1;
+      dlc = (m + 1) & ~1;
+      da = workspace(c, WS_STAGE_A, (size_t)dla * ca * sizeof(T));
+      db = workspace(c, WS_STAGE_B, (size_t)dlb * cb * sizeof(T));
+      dc = workspace(c, WS_STAGE_C, (size_t)dlc * n * sizeof(T));
+      if (!da || !db || !dc) st = B2_ERR_NOMEM;
+      cudaError_t e = cudaSuccess;
+      if (st == B2_OK)
+        e = cudaMemcpy2DAsync(da, (size_t)dla * sizeof(T), a, (size_t)lda * sizeof(T),
+                              (size_t)ra * sizeof(T), ca, cudaMemcpyDefault, c->h2d);
+      int issued = 0;
+      for (int j = 0; j < nb && st == B2_OK && e == cudaSuccess; ++j) {
+        const int j0 = j * cw, nj = (n - j0 < cw) ? n - j0 : cw;
+        const T *bh = notrans(tb) ? b + (size_t)j0 * ldb : b + j0;
+        T *bd = notrans(tb) ? (T *)db + (size_t)j0 * dlb : (T *)db + j0;
+        e = notrans(tb)
+                ? cudaMemcpy2DAsync(bd, (size_t)dlb * sizeof(T), bh, (size_t)ldb * sizeof(T),
+                                    (size_t)k * sizeof(T), nj, cudaMemcpyDefault, c->h2d)
+                : cudaMemcpy2DAsync(bd, (size_t)dlb * sizeof(T), bh, (size_t)ldb * sizeof(T),
+                                    (size_t)nj * sizeof(T), k, cudaMemcpyDefault, c->h2d);
+        T *cd = (T *)dc + (size_t)j0 * dlc;
+        T *ch = cm + (size_t)j0 * ldc;
+        if (e == cudaSuccess)
+          e = cudaMemcpy2DAsync(cd, (size_t)dlc * sizeof(T), ch, (size_t)ldc * sizeof(T),
+                                (size_t)m * sizeof(T), nj, cudaMemcpyDefault, c->h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[j], c->h2d);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->ev_in[j], 0);
+        if (e != cudaSuccess) break;
+        st = run((const T *)da, dla, (const T *)bd, dlb, cd, dlc, nj, s);
+        if (st != B2_OK) break;
+        e = cudaEventRecord(c->ev_done[j], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->d2h, c->ev_done[j], 0);
+        if (e == cudaSuccess)
+          e = cudaMemcpy2DAsync(ch, (size_t)ldc * sizeof(T), cd, (size_t)dlc * sizeof(T),
+                                (size_t)m * sizeof(T), nj, cudaMemcpyDefault, c->d2h);
+        ++issued;
+      }
+      if (st == B2_OK && e != cudaSuccess) st = cuda_fail(e, "pipelined staging");
+      // Every stream drains before returning, whatever failed.
+      cudaError_t e1 = cudaStreamSynchronize(c->h2d);
+      cudaError_t e2 = cudaStreamSynchronize(s);
+      cudaError_t e3 = cudaStreamSynchronize(c->d2h);
+      if (st == B2_OK && e1 != cudaSuccess) st = cuda_fail(e1, "copy-in stream");
+      if (st == B2_OK && e2 != cudaSuccess) st = cuda_fail(e2, "stream sync");
+      if (st == B2_OK && e3 != cudaSuccess) st = cuda_fail(e3, "copy-out stream");
+      (void)issued;
     }
-    if (st == B2_OK) st = stage_in(c, WS_STAGE_C, cm, m, n, ldc, sizeof(T), &dc, &dlc, s);
-    if (st == B2_OK) st = run((const T *)da, dla, (const T *)db, dlb, (T *)dc, dlc, s);
-    if (st == B2_OK) st = stage_out(cm, ldc, dc, dlc, m, n, sizeof(T), s);
   }
   if (st == B2_OK) {
     cudaError_t e = cudaStreamSynchronize(s);
@@ -395,8 +490,8 @@ void dgemm_(const char *transa, const char *transb, const int *m, const int *n, 
   const double al = *alpha, be = *beta;
   gemm_dropin<double>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
                       [&](const double *A, int la, const double *B, int lb, double *C, int lc,
-                          cudaStream_t s) {
-                        return dgemm_device(ta, tb, *m, *n, *k, al, A, la, B, lb, be, C, lc,
+                          int ncols, cudaStream_t s) {
+                        return dgemm_device(ta, tb, *m, ncols, *k, al, A, la, B, lb, be, C, lc,
                                             B2_METHOD_DEFAULT, 0, s);
                       });
 }
@@ -412,8 +507,8 @@ void sgemm_(const char *transa, const char *transb, const int *m, const int *n, 
   const float al = *alpha, be = *beta;
   gemm_dropin<float>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
                      [&](const float *A, int la, const float *B, int lb, float *C, int lc,
-                         cudaStream_t s) {
-                       return sgemm_device(ta, tb, *m, *n, *k, al, A, la, B, lb, be, C, lc,
+                         int ncols, cudaStream_t s) {
+                       return sgemm_device(ta, tb, *m, ncols, *k, al, A, la, B, lb, be, C, lc,
                                            B2_METHOD_DEFAULT, s);
                      });
 }

@@ -48,6 +48,11 @@ struct Ctx {
   int dgemm_slices = 0;
   int sgemm_method = B2_METHOD_FP32;
   int fp64_override = 0;      // non-zero: use fp64_cfg for every FP64 GEMM
+  // Host-operand pipeline of the drop-in GEMMs: copy-in and copy-out streams
+  // and one (copied-in, computed) event pair per column block.
+  static constexpr int PIPE_MAX = 32;
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  cudaEvent_t ev_in[PIPE_MAX] = {}, ev_done[PIPE_MAX] = {};
 };
 
 Ctx *ctx();                          // initialises on first use; nullptr if no device

@@ -46,6 +46,48 @@ def test_dgemm_dropin_host_parity(cuda, m, n, k, ta, tb):
         assert e <= TOL, (m, n, k, ta, tb, al, be, e)
 
 
+@pytest.mark.parametrize("method", ["fp64", "ozaki"])
+def test_dgemm_dropin_pipelined_host_operands(cuda, method):
+    """Host operands of a product >= 2^32 flops go through the column-block
+    copy/compute/copy pipeline; blocks of 256-multiples leave a ragged last
+    block here (n = 1800), and op(B) blocks are row blocks of B for 'T'."""
+    m, n, k = 1000, 1800, 1300
+    rng = np.random.default_rng(77)
+    u = np.finfo(np.float64).eps / 2
+    blas.set_dgemm_method(method, 0)
+    try:
+        for ta, tb in [("N", "N"), ("T", "T")]:
+            a, b, c, ar, br = _case(rng, np.float64, m, n, k, ta, tb)
+            c[5, 1700] = np.nan  # beta == 0 still multiplies C: NaN survives, as in the reference
+            ref = c.copy(order="F")
+            O.gemm(ta, tb, m, n, k, 1.25, a[:ar], b[:br], 0.0, ref[:m])
+            got = c.copy(order="F")
+            blas.dgemm(ta, tb, m, n, k, 1.25, a, a.shape[0], b, b.shape[0], 0.0, got,
+                       got.shape[0])
+            assert np.array_equal(got[m:], c[m:]), "padding rows of C were written"
+            assert np.isnan(got[5, 1700]) and np.isnan(ref[5, 1700])
+            fin = np.isfinite(ref[:m])
+            assert fin.sum() == m * n - 1
+            g, r = np.where(fin, got[:m], 0.0), np.where(fin, ref[:m], 0.0)
+            e = normalized(g, r, k, a[:ar], b[:br], u)
+            assert e <= TOL, (method, ta, tb, e)
+    finally:
+        blas.set_dgemm_method("fp64", 0)
+
+
+def test_sgemm_dropin_pipelined_host_operands(cuda):
+    m, n, k = 900, 2100, 1500
+    rng = np.random.default_rng(78)
+    u = np.finfo(np.float32).eps / 2
+    a, b, c, ar, br = _case(rng, np.float32, m, n, k, "N", "T")
+    ref = c.copy(order="F")
+    O.gemm("N", "T", m, n, k, 0.5, a[:ar], b[:br], 2.0, ref[:m])
+    got = c.copy(order="F")
+    blas.sgemm("N", "T", m, n, k, 0.5, a, a.shape[0], b, b.shape[0], 2.0, got, got.shape[0])
+    assert np.array_equal(got[m:], c[m:])
+    assert normalized(got[:m], ref[:m], k, a[:ar], b[:br], u) <= TOL
+
+
 @pytest.mark.parametrize("m,n,k", [(37, 53, 29), (513, 129, 1031), (1024, 1024, 1024)])
 def test_sgemm_dropin_host_parity(cuda, m, n, k):
     rng = np.random.default_rng(k)
