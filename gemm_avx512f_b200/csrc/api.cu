@@ -48,6 +48,7 @@ struct CtxOwner {
       if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
       if (c->ev_done[i]) cudaEventDestroy(c->ev_done[i]);
     }
+    if (c->plan_ev) cudaEventDestroy(c->plan_ev);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
   }
@@ -98,6 +99,11 @@ Ctx *ctx() {
       delete c;
       return nullptr;
     }
+  }
+  if (cudaEventCreateWithFlags(&c->plan_ev, cudaEventDisableTiming) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete c;
+    return nullptr;
   }
   c->dgemm_method = method_from_env(getenv("B2_METHOD"), B2_METHOD_FP64);
   c->sgemm_method = method_from_env(getenv("B2_SGEMM_METHOD"), B2_METHOD_FP32);

@@ -53,6 +53,7 @@ struct Ctx {
   static constexpr int PIPE_MAX = 32;
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_in[PIPE_MAX] = {}, ev_done[PIPE_MAX] = {};
+  cudaEvent_t plan_ev = nullptr;  // marks the copy-back of the last Ozaki modulus count
 };
 
 Ctx *ctx();                          // initialises on first use; nullptr if no device

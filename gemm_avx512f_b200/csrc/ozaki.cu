@@ -145,12 +145,13 @@ CrtTable make_table(int s) {
 // contiguous read, with 4 columns (128 B per thread) in flight.
 __global__ void __launch_bounds__(256)
     norm_partial_rows_kernel(const double *__restrict__ X, long long sk, int R, int K, int kchunk,
-                             bool vec, double *__restrict__ pmax, double *__restrict__ pssq) {
+                             bool vec, double *__restrict__ pmax, double *__restrict__ pssq,
+                             double *__restrict__ pl1) {
   const int chunk = blockIdx.y;
   const int k0 = chunk * kchunk, k1 = min(K, k0 + kchunk);
   const int r0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
   if (r0 >= R) return;
-  double sa[4] = {0.0, 0.0, 0.0, 0.0}, ma[4] = {0.0, 0.0, 0.0, 0.0};
+  double sa[4] = {0.0, 0.0, 0.0, 0.0}, ma[4] = {0.0, 0.0, 0.0, 0.0}, la[4] = {0.0, 0.0, 0.0, 0.0};
   const double *p = X + r0;
   if (vec && r0 + 3 < R) {
     int k = k0;
@@ -166,7 +167,11 @@ __global__ void __launch_bounds__(256)
       for (int j = 0; j < 4; ++j) {
         const double v[4] = {a[j][0].x, a[j][0].y, a[j][1].x, a[j][1].y};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) { sa[e] = fma(v[e], v[e], sa[e]); ma[e] = fmax(ma[e], fabs(v[e])); }
+        for (int e = 0; e < 4; ++e) {
+          sa[e] = fma(v[e], v[e], sa[e]);
+          ma[e] = fmax(ma[e], fabs(v[e]));
+          la[e] += fabs(v[e]);
+        }
       }
     }
     for (; k < k1; ++k) {
@@ -175,6 +180,7 @@ __global__ void __launch_bounds__(256)
         const double v = __ldg(p + (long long)k * sk + e);
         sa[e] = fma(v, v, sa[e]);
         ma[e] = fmax(ma[e], fabs(v));
+        la[e] += fabs(v);
       }
     }
   } else {
@@ -183,11 +189,13 @@ __global__ void __launch_bounds__(256)
         const double v = __ldg(p + (long long)k * sk + e);
         sa[e] = fma(v, v, sa[e]);
         ma[e] = fmax(ma[e], fabs(v));
+        la[e] += fabs(v);
       }
   }
   for (int e = 0; e < 4 && r0 + e < R; ++e) {
     pmax[(long long)chunk * R + r0 + e] = ma[e];
     pssq[(long long)chunk * R + r0 + e] = sa[e];
+    pl1[(long long)chunk * R + r0 + e] = la[e];
   }
 }
 
@@ -196,14 +204,14 @@ __global__ void __launch_bounds__(256)
 __global__ void __launch_bounds__(256)
     norm_partial_kcont_kernel(const double *__restrict__ X, long long sr, int R, int K,
                               int kchunk, bool vec, double *__restrict__ pmax,
-                              double *__restrict__ pssq) {
+                              double *__restrict__ pssq, double *__restrict__ pl1) {
   const int chunk = blockIdx.y;
   const int k0 = chunk * kchunk, k1 = min(K, k0 + kchunk);
   const int warps = blockDim.x >> 5, lane = threadIdx.x & 31;
   const int r = blockIdx.x * warps + (threadIdx.x >> 5);
   if (r >= R) return;
   const double *p = X + (long long)r * sr;
-  double sa[4] = {0.0, 0.0, 0.0, 0.0}, ma[4] = {0.0, 0.0, 0.0, 0.0};
+  double sa[4] = {0.0, 0.0, 0.0, 0.0}, ma[4] = {0.0, 0.0, 0.0, 0.0}, la = 0.0;
   if (vec && (k0 & 1) == 0) {
     int k = k0 + 2 * lane;
     for (; k + 193 < k1; k += 256) {
@@ -215,6 +223,7 @@ __global__ void __launch_bounds__(256)
         sa[j] = fma(a[j].x, a[j].x, sa[j]);
         sa[j] = fma(a[j].y, a[j].y, sa[j]);
         ma[j] = fmax(ma[j], fmax(fabs(a[j].x), fabs(a[j].y)));
+        la += fabs(a[j].x) + fabs(a[j].y);
       }
     }
     for (; k + 1 < k1; k += 64) {
@@ -222,17 +231,20 @@ __global__ void __launch_bounds__(256)
       sa[0] = fma(a.x, a.x, sa[0]);
       sa[0] = fma(a.y, a.y, sa[0]);
       ma[0] = fmax(ma[0], fmax(fabs(a.x), fabs(a.y)));
+      la += fabs(a.x) + fabs(a.y);
     }
     if (k < k1) {
       const double v = __ldg(p + k);
       sa[0] = fma(v, v, sa[0]);
       ma[0] = fmax(ma[0], fabs(v));
+      la += fabs(v);
     }
   } else {
     for (int k = k0 + lane; k < k1; k += 32) {
       const double v = __ldg(p + k);
       sa[0] = fma(v, v, sa[0]);
       ma[0] = fmax(ma[0], fabs(v));
+      la += fabs(v);
     }
   }
   double s = (sa[0] + sa[1]) + (sa[2] + sa[3]);
@@ -240,10 +252,12 @@ __global__ void __launch_bounds__(256)
   for (int o = 16; o > 0; o >>= 1) {
     s += __shfl_down_sync(0xffffffffu, s, o);
     mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+    la += __shfl_down_sync(0xffffffffu, la, o);
   }
   if (lane == 0) {
     pmax[(long long)chunk * R + r] = mx;
     pssq[(long long)chunk * R + r] = s;
+    pl1[(long long)chunk * R + r] = la;
   }
 }
 
@@ -266,33 +280,87 @@ __device__ __forceinline__ void ssq_add(Ssq &a, double x) {
   a.s = fma(y, y, a.s);
 }
 
+// Exponent of a row outside the fast range (or holding Inf/NaN), from the
+// power-of-two-scaled sum of squares.
+__device__ int norm_slow_sigma(const double *p, long long sk, int K, int H) {
+  Ssq a{-2000, 0.0, 0};
+  for (int k = 0; k < K; ++k) ssq_add(a, p[(long long)k * sk]);
+  if (a.bad) return NONFINITE;
+  if (a.s == 0.0) return 0;
+  int g;
+  frexp(a.s * (1.0 + 0x1p-30), &g);
+  return H - (a.e + ((g + 1) >> 1));
+}
+
 // sigma_r = H - ceil(log2 ||x_r||_2); NONFINITE if the row holds Inf/NaN;
-// 0 for an all-zero row.
+// 0 for an all-zero row.  With `stat` non-null it also adds each finite
+// nonzero fast-range row's flatness log2(||x_r||_1 / (sqrt(K) ||x_r||_2)) to
+// stat[0] and the row count to stat[1] (the modulus-count statistic; about
+// -0.2 for uniform rows, far below -2 when a few elements carry the norm).
 __global__ void norm_finalize_kernel(const double *__restrict__ pmax,
-                                     const double *__restrict__ pssq, int R, int chunks, int H,
+                                     const double *__restrict__ pssq,
+                                     const double *__restrict__ pl1, int R, int chunks, int H,
                                      int *__restrict__ sigma, const double *__restrict__ X,
-                                     long long sr, long long sk, int K) {
+                                     long long sr, long long sk, int K, double *stat) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= R) return;
-  double mx = 0.0, ss = 0.0;
-  for (int c = 0; c < chunks; ++c) {
-    mx = fmax(mx, pmax[(long long)c * R + r]);
-    ss += pssq[(long long)c * R + r];
+  double flat = 0.0, cnt = 0.0;
+  if (r < R) {
+    double mx = 0.0, ss = 0.0, l1 = 0.0;
+#pragma unroll 8
+    for (int c = 0; c < chunks; ++c) {
+      mx = fmax(mx, pmax[(long long)c * R + r]);
+      ss += pssq[(long long)c * R + r];
+      l1 += pl1[(long long)c * R + r];
+    }
+    if (mx == 0.0 && ss == 0.0) {
+      sigma[r] = 0;
+    } else if (isfinite(ss) && mx >= 0x1p-480 && mx <= 0x1p480) {
+      int g;
+      frexp(ss * (1.0 + 0x1p-30), &g);  // ss (1+eps) < 2^g, so ||x|| < 2^ceil(g/2)
+      sigma[r] = H - ((g + 1) >> 1);
+      flat = log2(l1 / (sqrt((double)K) * sqrt(ss)));
+      cnt = 1.0;
+    } else {
+      sigma[r] = norm_slow_sigma(X + (long long)r * sr, sk, K, H);
+    }
   }
-  if (mx == 0.0 && ss == 0.0) { sigma[r] = 0; return; }
-  int g, e = 0;
-  if (isfinite(ss) && mx >= 0x1p-480 && mx <= 0x1p480) {
-    frexp(ss * (1.0 + 0x1p-30), &g);  // ss (1+eps) < 2^g, so ||x|| < 2^ceil(g/2)
-  } else {
-    Ssq a{-2000, 0.0, 0};
-    const double *p = X + (long long)r * sr;
-    for (int k = 0; k < K; ++k) ssq_add(a, p[(long long)k * sk]);
-    if (a.bad) { sigma[r] = NONFINITE; return; }
-    if (a.s == 0.0) { sigma[r] = 0; return; }
-    frexp(a.s * (1.0 + 0x1p-30), &g);
-    e = a.e;
+  if (stat) {  // every lane of every warp reaches this point (no early return)
+    for (int o = 16; o > 0; o >>= 1) {
+      flat += __shfl_down_sync(0xffffffffu, flat, o);
+      cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    }
+    if ((threadIdx.x & 31) == 0 && cnt > 0.0) {
+      atomicAdd(stat, flat);
+      atomicAdd(stat + 1, cnt);
+    }
   }
-  sigma[r] = H - (e + ((g + 1) >> 1));
+}
+
+// Modulus count of the call, written to *s_dev for the slice, GEMM and
+// reconstruction kernels.  Adaptive calls take s_hi when the mean row
+// flatness of op(A) plus that of op(B) is below log2_rho_min (heavy-tailed
+// rows: a few elements carry each norm, so the truncation error, relative to
+// the norms, grows against |C| and against FP64's own error) and then raise
+// every finite exponent by dH = H(s_hi) - H(s_base); otherwise s_base.  One
+// block.
+__global__ void ozaki_decide_kernel(const double *statA, const double *statB, int adaptive,
+                                    int s_base, int s_hi, int dH, double log2_rho_min,
+                                    int *s_dev, int *sigA, int m, int *tauB, int n) {
+  __shared__ int s_eff;
+  if (threadIdx.x == 0) {
+    int sv = s_base;
+    if (adaptive && statA[1] > 0.0 && statB[1] > 0.0 &&
+        statA[0] / statA[1] + statB[0] / statB[1] < log2_rho_min)
+      sv = s_hi;
+    s_eff = sv;
+    *s_dev = sv;
+  }
+  __syncthreads();
+  if (s_eff == s_base) return;
+  for (int i = threadIdx.x; i < m + n; i += blockDim.x) {
+    int *q = i < m ? sigA + i : tauB + (i - m);
+    if (*q != NONFINITE) *q += dH;
+  }
 }
 
 // --------------------------------------------------------- residue slices --
@@ -364,8 +432,8 @@ __device__ __forceinline__ double pow2(int e) {  // e in [-1022, 1023]
 template <bool ROWCONT>
 __global__ void __launch_bounds__(256)
     slice_kernel(const double *__restrict__ X, long long sr, long long sk, int R, int K,
-                 const int *__restrict__ sigma, int s, int8_t *__restrict__ out, long long kp,
-                 long long plane) {
+                 const int *__restrict__ sigma, const int *__restrict__ s_dev,
+                 int8_t *__restrict__ out, long long kp, long long plane) {
   __shared__ double tile[32][65];
   const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32;
   const int tid = threadIdx.x;
@@ -398,7 +466,7 @@ __global__ void __launch_bounds__(256)
     c2[j] = (unsigned)(u >> 42);
   }
   const int nk = min(8, K - (k0 + kg));
-  store_slices<0>(c0, c1, c2, s, out + (long long)r * kp + k0 + kg, plane, nk);
+  store_slices<0>(c0, c1, c2, *s_dev, out + (long long)r * kp + k0 + kg, plane, nk);
 }
 
 // ---------------------------------------------------------- GEMM epilogue --
@@ -470,13 +538,15 @@ __device__ __forceinline__ double byte_to_double(unsigned b) {  // exact, no con
 // Rows/columns flagged NONFINITE use a direct FP64 dot product.
 template <int LIMBS>
 __global__ void __launch_bounds__(256)
-    reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr, int s, int M,
+    reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr, int s,
+                       const int *__restrict__ s_dev, int M,
                        int N, const int *__restrict__ sigA, const int *__restrict__ tauB,
                        double alpha, double beta, double *__restrict__ C, int ldc,
                        const double *__restrict__ A, long long asr, long long ask,
                        const double *__restrict__ B, long long bsk, long long bsc, int K) {
   static_assert(LIMBS == 3 || LIMBS == 4, "3 x 40-bit or 4 x 32-bit limbs");
   constexpr int LB = LIMBS == 3 ? 40 : 32;
+  if (*s_dev != s) return;  // the launch for the other count does this call
   // Grid: x covers the rows m in groups of 4 per thread, y strides over the
   // columns n (no integer division per item).
   const int m0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
@@ -581,21 +651,42 @@ __global__ void __launch_bounds__(256)
 }
 
 // Launch of the reconstruction with the limb width the modulus count allows.
-void launch_reconstruct(const uint8_t *R, long long plane, int ldr, int s, int M, int N,
+void launch_reconstruct(const uint8_t *R, long long plane, int ldr, const int *s_dev, int s_lo,
+                        int s_hi, int M, int N,
                         const int *sigA, const int *tauB, double alpha, double beta, double *C,
                         int ldc, const double *A, long long asr, long long ask, const double *B,
                         long long bsk, long long bsc, int K, cudaStream_t st) {
   const dim3 blocks((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)(N < 65535 ? N : 65535));
-  if (s <= 15)
-    reconstruct_kernel<3><<<blocks, 256, 0, st>>>(R, plane, ldr, s, M, N, sigA, tauB, alpha, beta,
-                                                   C, ldc, A, asr, ask, B, bsk, bsc, K);
+  // one launch per possible count (s_lo, and s_hi when it differs); each
+  // returns at once unless the device-chosen count is its own
+  if (s_lo <= 15)
+    reconstruct_kernel<3><<<blocks, 256, 0, st>>>(R, plane, ldr, s_lo, s_dev, M, N, sigA, tauB,
+                                                   alpha, beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
   else
-    reconstruct_kernel<4><<<blocks, 256, 0, st>>>(R, plane, ldr, s, M, N, sigA, tauB, alpha, beta,
-                                                   C, ldc, A, asr, ask, B, bsk, bsc, K);
+    reconstruct_kernel<4><<<blocks, 256, 0, st>>>(R, plane, ldr, s_lo, s_dev, M, N, sigA, tauB,
+                                                   alpha, beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
+  if (s_hi != s_lo) {
+    // The heavy-tail count is the rare one: this launch usually exits at
+    // once, and a grid of about 8 blocks per SM (columns strided) keeps that
+    // cheap.
+    dim3 b4 = blocks;
+    {
+      const unsigned y = 1184u / (blocks.x > 0 ? blocks.x : 1u);
+      b4.y = y < 1u ? 1u : (y < blocks.y ? y : blocks.y);
+    }
+    if (s_hi <= 15)
+      reconstruct_kernel<3><<<b4, 256, 0, st>>>(R, plane, ldr, s_hi, s_dev, M, N, sigA, tauB, alpha,
+                                                beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
+    else
+      reconstruct_kernel<4><<<b4, 256, 0, st>>>(R, plane, ldr, s_hi, s_dev, M, N, sigA, tauB, alpha,
+                                                beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
+  }
 }
 
 struct OzPlan {
   int s = 0, kchunks = 0;
+  const int *word = nullptr;  // pinned copy of the device-chosen count (behind ev)
+  cudaEvent_t ev = nullptr;
 };
 thread_local OzPlan g_last_plan;
 
@@ -656,7 +747,7 @@ thread_local int g_oz_variant = default_oz_variant();
 
 int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, int n, int m, int s,
                 long long kp, long long planeX, long long planeY, const ResidueEpi &epi,
-                int device, int sm_count, int *derr, cudaStream_t st) {
+                int device, int sm_count, int *derr, cudaStream_t st, const int *s_dev) {
   const int ybox = variant == 0 ? 256 : 128;  // pair variants stage BN/2 = 128 rows per CTA
   CUtensorMap tmX, tmY;
   int rc = umma::make_kmajor_map(&tmX, umma::KIND_I8, X, kcl, n, s, kp, planeX, umma::BM);
@@ -665,19 +756,19 @@ int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, in
   switch (variant) {
     case 1:
       return umma::launch<umma::KIND_I8, 128, 6>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
-                                                  "ozaki_i8_gemm");
+                                                  "ozaki_i8_gemm", 0, s_dev);
     case 2:
       return umma::launch<umma::KIND_I8, 128, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
-                                                  "ozaki_i8_gemm");
+                                                  "ozaki_i8_gemm", 0, s_dev);
     case 3:
       return umma::launch_pair<umma::KIND_I8, 256, 6>(tmX, tmY, n, m, kcl, s, epi, device, derr,
-                                                       st, "ozaki_i8_gemm");
+                                                       st, "ozaki_i8_gemm", s_dev);
     case 4:
       return umma::launch_pair<umma::KIND_I8, 256, 7>(tmX, tmY, n, m, kcl, s, epi, device, derr,
-                                                       st, "ozaki_i8_gemm");
+                                                       st, "ozaki_i8_gemm", s_dev);
     default:
       return umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
-                                                  "ozaki_i8_gemm");
+                                                  "ozaki_i8_gemm", 0, s_dev);
   }
 }
 
@@ -705,24 +796,25 @@ int norm_chunks(int R, int K, bool rowcont) {
 }
 
 int norm_exponents(const double *X, long long sr, long long sk, int R, int K, int H, int *sigma,
-                   void *scratch, cudaStream_t s) {
+                   void *scratch, double *stat, cudaStream_t s) {
   const bool rowcont = sr == 1;
   const int want = norm_chunks(R, K, rowcont);
   const int kchunk = K > 0 ? (int)round_up((K + want - 1) / want, 8) : 8;
   const int chunks = K > 0 ? (K + kchunk - 1) / kchunk : 1;
   double *pmax = (double *)round_up((uintptr_t)scratch, 16);
   double *pssq = pmax + (long long)chunks * R;
+  double *pl1 = pssq + (long long)chunks * R;
   if (rowcont) {
     const bool vec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && ((sk & 1) == 0);
     dim3 grid((R + 1023) / 1024, chunks);
     B2_PROF("ozaki_norm_rowcont", s);
-    norm_partial_rows_kernel<<<grid, 256, 0, s>>>(X, sk, R, K, kchunk, vec, pmax, pssq);
+    norm_partial_rows_kernel<<<grid, 256, 0, s>>>(X, sk, R, K, kchunk, vec, pmax, pssq, pl1);
   } else {
     const bool vec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && ((sr & 1) == 0) && sk == 1;
     dim3 grid((R + 7) / 8, chunks);
     B2_PROF("ozaki_norm_kcont", s);
     if (sk == 1) {
-      norm_partial_kcont_kernel<<<grid, 256, 0, s>>>(X, sr, R, K, kchunk, vec, pmax, pssq);
+      norm_partial_kcont_kernel<<<grid, 256, 0, s>>>(X, sr, R, K, kchunk, vec, pmax, pssq, pl1);
     } else {
       return B2_ERR_ARG;  // every operand view has one unit stride
     }
@@ -730,8 +822,8 @@ int norm_exponents(const double *X, long long sr, long long sk, int R, int K, in
   B2_CUDA_TRY(cudaGetLastError());
   {
     B2_PROF("ozaki_norm_finalize", s);
-    norm_finalize_kernel<<<(R + 255) / 256, 256, 0, s>>>(pmax, pssq, R, chunks, H, sigma, X, sr,
-                                                          sk, K);
+    norm_finalize_kernel<<<(R + 255) / 256, 256, 0, s>>>(pmax, pssq, pl1, R, chunks, H, sigma, X,
+                                                          sr, sk, K, stat);
   }
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
@@ -739,7 +831,7 @@ int norm_exponents(const double *X, long long sr, long long sk, int R, int K, in
 
 size_t norm_scratch_bytes(int R, int K) {
   const int a = norm_chunks(R, K, true), b = norm_chunks(R, K, false);
-  return (size_t)(a > b ? a : b) * R * 16 + 64;
+  return (size_t)(a > b ? a : b) * R * 24 + 64;
 }
 
 }  // namespace
@@ -761,6 +853,11 @@ int ozaki_auto_moduli(int k) {
   return 15;
 }
 
+// Heavy-tail threshold of the automatic modulus count: 16 moduli instead of 15
+// when the mean log2 row flatness of op(A) plus that of op(B) is below -4
+// (uniform data: about -0.4; a = u exp(g): about -1.9; a = u exp(4g): about -10).
+constexpr double OZ_LOG2_RHO_MIN = -4.0;
+
 int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
                 const double *B, int ldb, double beta, double *C, int ldc, int slices,
                 cudaStream_t st) {
@@ -768,11 +865,16 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   Ctx *cx = ctx();
   if (!cx) return B2_ERR_NO_DEVICE;
   if (k <= 0 || alpha == 0.0) return beta == 1.0 ? B2_OK : scale_matrix_d(m, n, beta, C, ldc, st);
-  const int s = slices > 0 ? slices : ozaki_auto_moduli(k);
-  if (s < 2 || s > OZ_MAX) return B2_ERR_ARG;
+  // slices <= 0: automatic count, s_base or (heavy-tailed inputs) s_base + 1,
+  // chosen on the device after the norm pass; buffers are sized for s_max.
+  const bool adaptive = slices <= 0;
+  const int s_base = adaptive ? ozaki_auto_moduli(k) : slices;
+  if (s_base < 2 || s_base > OZ_MAX) return B2_ERR_ARG;
+  const int s_max = adaptive && s_base < OZ_MAX ? s_base + 1 : s_base;
   int rc = upload_tables(cx->device, st);
   if (rc != B2_OK) return rc;
-  const CrtTable t = make_table(s);
+  const CrtTable t = make_table(s_base);
+  const int dH = make_table(s_max).H - t.H;
 
   const bool tA = !(ta == 'N' || ta == 'n');
   const bool tB = !(tb == 'N' || tb == 'n');
@@ -788,21 +890,35 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   const long long planeY = (long long)m * kp, planeX = (long long)n * kp;
   const long long planeR = (long long)n * mp;
 
-  int8_t *Y = (int8_t *)workspace(cx, WS_OZ_Y, (size_t)planeY * s);
-  int8_t *X = (int8_t *)workspace(cx, WS_OZ_X, (size_t)planeX * s);
-  uint8_t *Rb = (uint8_t *)workspace(cx, WS_OZ_R, (size_t)planeR * s);
+  int8_t *Y = (int8_t *)workspace(cx, WS_OZ_Y, (size_t)planeY * s_max);
+  int8_t *X = (int8_t *)workspace(cx, WS_OZ_X, (size_t)planeX * s_max);
+  uint8_t *Rb = (uint8_t *)workspace(cx, WS_OZ_R, (size_t)planeR * s_max);
   const size_t nsA = norm_scratch_bytes(m, k), nsB = norm_scratch_bytes(n, k);
-  const size_t sc_bytes = round_up((m + n) * sizeof(int), 256) + nsA + nsB + 512;
+  // [sigma|tau][stat A (2 doubles), stat B (2 doubles), modulus count][norm A][norm B]
+  const size_t o_stat = round_up((m + n) * sizeof(int), 256);
+  const size_t o_scr = o_stat + 256;
+  const size_t sc_bytes = o_scr + round_up(nsA, 256) + nsB + 512;
   uint8_t *sc = (uint8_t *)workspace(cx, WS_OZ_SCALE, sc_bytes);
   if (!Y || !X || !Rb || !sc) return B2_ERR_NOMEM;
   int *sigA = (int *)sc;
   int *tauB = sigA + m;
-  void *scrA = sc + round_up((m + n) * sizeof(int), 256);
+  double *stat = (double *)(sc + o_stat);
+  int *s_dev = (int *)(stat + 4);
+  void *scrA = sc + o_scr;
   void *scrB = (uint8_t *)scrA + round_up(nsA, 256);
 
-  rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, st);
-  if (rc == B2_OK) rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, scrB, st);
+  if (adaptive) B2_CUDA_TRY(cudaMemsetAsync(stat, 0, 4 * sizeof(double), st));
+  rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
+  if (rc == B2_OK)
+    rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, scrB, adaptive ? stat + 2 : nullptr, st);
   if (rc != B2_OK) return rc;
+  {
+    B2_PROF("ozaki_decide", st);
+    ozaki_decide_kernel<<<1, 1024, 0, st>>>(stat, stat + 2, adaptive && s_max > s_base ? 1 : 0,
+                                            s_base, s_max, dH, OZ_LOG2_RHO_MIN, s_dev, sigA, m,
+                                            tauB, n);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
 
   for (int c = 0; c < kchunks && rc == B2_OK; ++c) {
     const int kc0 = c * KCH, kcl = (k - kc0 < KCH) ? k - kc0 : KCH;
@@ -810,33 +926,44 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
       dim3 grid((kcl + 63) / 64, (m + 31) / 32);
       B2_PROF(asr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
       if (asr == 1)
-        slice_kernel<true><<<grid, 256, 0, st>>>(A + kc0 * ask, asr, ask, m, kcl, sigA, s, Y, kp, planeY);
+        slice_kernel<true><<<grid, 256, 0, st>>>(A + kc0 * ask, asr, ask, m, kcl, sigA, s_dev, Y,
+                                                 kp, planeY);
       else
-        slice_kernel<false><<<grid, 256, 0, st>>>(A + kc0 * ask, asr, ask, m, kcl, sigA, s, Y, kp, planeY);
+        slice_kernel<false><<<grid, 256, 0, st>>>(A + kc0 * ask, asr, ask, m, kcl, sigA, s_dev, Y,
+                                                  kp, planeY);
       B2_CUDA_TRY(cudaGetLastError());
     }
     {
       dim3 grid((kcl + 63) / 64, (n + 31) / 32);
       B2_PROF(bsr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
       if (bsr == 1)
-        slice_kernel<true><<<grid, 256, 0, st>>>(B + kc0 * bsk, bsr, bsk, n, kcl, tauB, s, X, kp, planeX);
+        slice_kernel<true><<<grid, 256, 0, st>>>(B + kc0 * bsk, bsr, bsk, n, kcl, tauB, s_dev, X,
+                                                 kp, planeX);
       else
-        slice_kernel<false><<<grid, 256, 0, st>>>(B + kc0 * bsk, bsr, bsk, n, kcl, tauB, s, X, kp, planeX);
+        slice_kernel<false><<<grid, 256, 0, st>>>(B + kc0 * bsk, bsr, bsk, n, kcl, tauB, s_dev, X,
+                                                  kp, planeX);
       B2_CUDA_TRY(cudaGetLastError());
     }
     ResidueEpi epi{Rb, planeR, (int)mp, n, m, c > 0 ? 1 : 0};
-    rc = run_i8_gemm(g_oz_variant, X, Y, kcl, n, m, s, kp, planeX, planeY, epi, cx->device,
-                     cx->sm_count, cx->derr, st);
+    rc = run_i8_gemm(g_oz_variant, X, Y, kcl, n, m, s_max, kp, planeX, planeY, epi, cx->device,
+                     cx->sm_count, cx->derr, st, s_dev);
   }
   if (rc != B2_OK) return rc;
   {
     B2_PROF("ozaki_reconstruct", st);
-    launch_reconstruct(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha, beta, C, ldc, A, asr, ask,
-                       B, bsk, bsr, k, st);
+    launch_reconstruct(Rb, planeR, (int)mp, s_dev, s_base, s_max, m, n, sigA, tauB, alpha, beta, C,
+                       ldc, A, asr, ask, B, bsk, bsr, k, st);
     B2_CUDA_TRY(cudaGetLastError());
   }
-  g_last_plan.s = s;
+  // The count actually used is known on the device only: copy it to pinned
+  // memory behind an event, read by b2_ozaki_last_plan.
+  int *plan_word = (int *)((uint8_t *)cx->pinned + 64);
+  B2_CUDA_TRY(cudaMemcpyAsync(plan_word, s_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B2_CUDA_TRY(cudaEventRecord(cx->plan_ev, st));
+  g_last_plan.s = s_base;
   g_last_plan.kchunks = kchunks;
+  g_last_plan.word = plan_word;
+  g_last_plan.ev = cx->plan_ev;
   return B2_OK;
 }
 
@@ -844,6 +971,8 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
 
 extern "C" int b2_ozaki_last_plan(int *out, int n) {
   if (!out || n < 2) return B2_ERR_ARG;
+  if (b2::g_last_plan.ev && cudaEventSynchronize(b2::g_last_plan.ev) == cudaSuccess)
+    b2::g_last_plan.s = *b2::g_last_plan.word;
   out[0] = b2::g_last_plan.s;
   out[1] = b2::g_last_plan.kchunks;
   return B2_OK;
@@ -948,6 +1077,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   rc = noalloc_base(dev, &base);
   if (rc != B2_OK) return rc;
   int *derr = (int *)base;
+  int *s_dev = (int *)(base + 64);  // modulus count read by the kernels (set below)
   int *sigA = (int *)(base + o_sig);
   int *tauB = sigA + m;
   int8_t *Y = (int8_t *)(base + o_Y);
@@ -964,23 +1094,27 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   const long long asr = tA ? lda : 1, ask = tA ? 1 : lda;
   const long long bsr = tB ? 1 : ldb, bsk = tB ? ldb : 1;
 
-  rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, base + o_nA, st);
-  if (rc == B2_OK) rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, base + o_nB, st);
+  rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, base + o_nA, nullptr, st);
+  if (rc == B2_OK) rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, base + o_nB, nullptr, st);
   if (rc != B2_OK) return rc;
+  // fixed count (no statistics): the kernel only stores s
+  ozaki_decide_kernel<<<1, 32, 0, st>>>(nullptr, nullptr, 0, s, s, 0, 0.0, s_dev, sigA, m, tauB,
+                                        n);
+  B2_CUDA_TRY(cudaGetLastError());
   {
     dim3 grid((k + 63) / 64, (m + 31) / 32);
     if (asr == 1)
-      slice_kernel<true><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s, Y, kp, planeY);
+      slice_kernel<true><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s_dev, Y, kp, planeY);
     else
-      slice_kernel<false><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s, Y, kp, planeY);
+      slice_kernel<false><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s_dev, Y, kp, planeY);
     B2_CUDA_TRY(cudaGetLastError());
   }
   {
     dim3 grid((k + 63) / 64, (n + 31) / 32);
     if (bsr == 1)
-      slice_kernel<true><<<grid, 256, 0, st>>>(B, bsr, bsk, n, k, tauB, s, X, kp, planeX);
+      slice_kernel<true><<<grid, 256, 0, st>>>(B, bsr, bsk, n, k, tauB, s_dev, X, kp, planeX);
     else
-      slice_kernel<false><<<grid, 256, 0, st>>>(B, bsr, bsk, n, k, tauB, s, X, kp, planeX);
+      slice_kernel<false><<<grid, 256, 0, st>>>(B, bsr, bsk, n, k, tauB, s_dev, X, kp, planeX);
     B2_CUDA_TRY(cudaGetLastError());
   }
   CUtensorMap tmX, tmY;
@@ -991,7 +1125,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   rc = umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, k, s, epi, prop.multiProcessorCount,
                                             derr, st, "ozaki_i8_gemm");
   if (rc != B2_OK) return rc;
-  launch_reconstruct(Rb, planeR, (int)mp, s, m, n, sigA, tauB, alpha, beta, C, ldc, A, asr, ask, B,
+  launch_reconstruct(Rb, planeR, (int)mp, s_dev, s, s, m, n, sigA, tauB, alpha, beta, C, ldc, A, asr, ask, B,
                      bsk, bsr, k, st);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;

@@ -196,6 +196,7 @@ struct Problem {
   int P, Q;        // rows of X and of Y (output tile space P x Q)
   int kblocks;     // K extent in 128-byte blocks
   int nbatch;      // independent products (3-D tensor maps, batch = outer coordinate)
+  const int *nbatch_dev;  // if set: the batch count actually run (<= nbatch), read on the device
   int tiles_p, tiles_q;
   int group;       // tile rasterisation: GROUP rows of P tiles share a sweep over Q
   int *derr;       // device error word
@@ -245,7 +246,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int *abort_flag = reinterpret_cast<volatile int *>(gbase + L::BAR_OFF + L::BAR_BYTES + 8);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int total_tiles = pr.tiles_p * pr.tiles_q * pr.nbatch;
+  const int nbatch = pr.nbatch_dev ? min(*pr.nbatch_dev, pr.nbatch) : pr.nbatch;
+  const int total_tiles = pr.tiles_p * pr.tiles_q * nbatch;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -516,7 +518,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   const uint32_t rank = cluster_rank();
   const bool leader = rank == 0;
   const int pair = (int)cluster_id_x(), npairs = (int)cluster_count_x();
-  const int total_tiles = pr.tiles_p * pr.tiles_q * pr.nbatch;
+  const int nbatch = pr.nbatch_dev ? min(*pr.nbatch_dev, pr.nbatch) : pr.nbatch;
+  const int total_tiles = pr.tiles_p * pr.tiles_q * nbatch;
   const uint32_t peer_abort = map_rank(smem_u32((const void *)abort_flag), rank ^ 1u);
 
   if (threadIdx.x == 0) {
@@ -684,13 +687,14 @@ int make_kmajor_map(CUtensorMap *map, int kind, const void *base, long long kele
 template <int KIND, int BN, int STAGES, class Epi>
 int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
            int nbatch, const Epi &epi, int sm_count, int *derr, cudaStream_t s,
-           const char *prof_name, int max_ctas = 0) {
+           const char *prof_name, int max_ctas = 0, const int *nbatch_dev = nullptr) {
   using L = SmemLayout<BN, STAGES>;
   Problem pr;
   pr.P = P;
   pr.Q = Q;
   pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
   pr.nbatch = nbatch;
+  pr.nbatch_dev = nbatch_dev;
   pr.tiles_p = (P + BM - 1) / BM;
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;
@@ -715,13 +719,14 @@ int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long lo
 template <int KIND, int BN, int STAGES, class Epi>
 int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
                 int nbatch, const Epi &epi, int device, int *derr, cudaStream_t s,
-                const char *prof_name) {
+                const char *prof_name, const int *nbatch_dev = nullptr) {
   using L = SmemLayout<BN / 2, STAGES>;
   Problem pr;
   pr.P = P;
   pr.Q = Q;
   pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
   pr.nbatch = nbatch;
+  pr.nbatch_dev = nbatch_dev;
   pr.tiles_p = (P + PAIR_BM - 1) / PAIR_BM;
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;

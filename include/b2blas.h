@@ -127,7 +127,9 @@ B2_API int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha,
              int slices, void *stream);
 
 /* Plan of the last Ozaki DGEMM on this thread: out[0] = modulus (slice)
- * count, out[1] = number of K chunks (K is cut at 65536 per exact INT32 pass). */
+ * count, out[1] = number of K chunks (K is cut at 65536 per exact INT32 pass).
+ * With slices = 0 the count (15, or 16 for heavy-tailed rows) is chosen on the
+ * device; this call waits for that choice to be copied back. */
 B2_API int b2_ozaki_last_plan(int *out, int n);
 
 /* Allocation-free INT8 Ozaki DGEMM.  No counterpart in the reference: it is
@@ -135,7 +137,8 @@ B2_API int b2_ozaki_last_plan(int *out, int n);
  * during CUDA graph capture, real-time loops that must stay out of the
  * allocator, processes whose device memory is reserved up front).  Same
  * contract and result as b2_dgemm(..., B2_METHOD_OZAKI, slices, stream) on
- * device pointers, but all scratch lives in one static device array of
+ * device pointers (slices 0 means 15 moduli here: the heavy-tail switch to 16
+ * of the allocating path is not made), but all scratch lives in one static device array of
  * B2_NOALLOC_SCRATCH_BYTES per device, reserved when the library loads and
  * held until exit; the call never allocates or frees.  Problems whose scratch
  * exceeds that maximum (about 1200^3 at 15 moduli; K <= 65536) return

@@ -155,9 +155,31 @@ def test_error_within_2x_of_fp64(cuda, phi):
     A, B = (torch.from_numpy(x).to(cuda) for x in (a, b))
     C = torch.zeros(n * n, dtype=torch.float64, device=cuda)
     errs = {}
+    plan = (__import__("ctypes").c_int * 2)()
     for meth in ("fp64", "ozaki"):
         out = C.clone()
         blas.dgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, out, n, method=meth)
+        if meth == "ozaki":
+            _lib.lib().b2_ozaki_last_plan(plan, 2)
         errs[meth] = blas.dgemm_error_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, out, n)
+    # automatic count: 15 moduli, 16 for heavy-tailed rows (phi = 4)
+    assert plan[0] == (16 if phi >= 4 else 15), (phi, plan[0])
     assert errs["ozaki"][0] <= 2.0 * errs["fp64"][0], errs
     assert _lib.lib().b2_device_error(0) == 0
+
+
+def test_explicit_modulus_count_is_kept_for_heavy_tails(cuda):
+    import torch
+
+    n = 512
+    rng = np.random.default_rng(12)
+    a = rng.uniform(-1, 1, n * n) * np.exp(4.0 * rng.standard_normal(n * n))
+    b = rng.uniform(-1, 1, n * n) * np.exp(4.0 * rng.standard_normal(n * n))
+    A, B = (torch.from_numpy(x).to(cuda) for x in (a, b))
+    plan = (__import__("ctypes").c_int * 2)()
+    for s in (14, 15):
+        out = torch.zeros(n * n, dtype=torch.float64, device=cuda)
+        blas.dgemm_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, out, n, method="ozaki",
+                          slices=s)
+        _lib.lib().b2_ozaki_last_plan(plan, 2)
+        assert plan[0] == s
