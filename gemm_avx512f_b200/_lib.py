@@ -89,6 +89,12 @@ def lib() -> C.CDLL:
     L.b2_dtrsm.argtypes = [ch, ch, ch, ch, i, i, d, p, i, p, i, i, i, p]
     L.b2_zgemm3m.argtypes = [ch, ch, i, i, i, p, p, i, p, i, p, p, i, p]
     L.b2_cgemm3m.argtypes = [ch, ch, i, i, i, p, p, i, p, i, p, p, i, p]
+    lg = C.c_long
+    L.b2_dgemm_kernel.argtypes = [i, i, lg, lg, lg, d, p, p, p, lg, p]
+    L.b2_sgemm_kernel.argtypes = [i, i, lg, lg, lg, f, p, p, p, lg, p]
+    L.b2_zgemm3m_kernel.argtypes = [i, i, lg, lg, lg, d, d, p, p, p, lg, p]
+    L.b2_cgemm3m_kernel.argtypes = [i, i, lg, lg, lg, f, f, p, p, p, lg, p]
+    L.b2_dtrsm_kernel.argtypes = [ch, ch, lg, lg, p, p, p, lg, lg, p]
     L.b2_dgemm_error.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, p, i, pd, pd, p]
     L.b2_device_error.argtypes = [i]
     L.b2_dgemm_ozaki_noalloc.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, p]

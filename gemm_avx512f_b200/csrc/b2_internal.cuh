@@ -32,6 +32,7 @@ enum WsSlot {
   WS_OZ_X, WS_OZ_Y, WS_OZ_R, WS_OZ_SCALE,   // Ozaki slices / residues / exponents
   WS_SPLIT_X, WS_SPLIT_Y,                   // SGEMM split planes
   WS_TRSM, WS_TRSM_INV, WS_TRSM_TMP, WS_3M, WS_GROUP, WS_ERR, WS_MISC,
+  WS_KABI_A, WS_KABI_B, WS_KABI_D,         // kernel-ABI unpacked panels / 3M product
   WS_COUNT
 };
 

@@ -181,6 +181,45 @@ B2_API int b2_cgemm3m(char transa, char transb, int m, int n, int k, const float
                int ldc, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* OpenBLAS kernel-level ABI on device pointers: what an OpenBLAS-style       */
+/* level-3 driver calls on its packed blocks.  Packed layout (the reference's */
+/* copy routines, OpenBLAS-like_implementation/dgemm.c:304-403): an operand   */
+/* of R rows (rows of A, columns of B) and depth k is cut into full panels of */
+/* `unroll` rows, then panels of unroll/2, unroll/4, ..., 1; a panel of width */
+/* w starting at row r0 sits at offset r0*k and holds (r, kk) at              */
+/* r0*k + kk*w + (r - r0).  Unrolls are powers of two <= 64.  All pointers    */
+/* are device memory; the calls are asynchronous on `stream` (NULL = the      */
+/* library stream) and return a b2_status.                                   */
+/* ------------------------------------------------------------------------ */
+
+/* C (m x n, ldc) += alpha * A * B on packed A (unroll_m) and B (unroll_n):
+ * the CNAME kernels of dgemm.c:247-263 (16x2), dgemm_kernel_4x8_skylakex_2.c:
+ * 661-668 (4x8), kernel_avx512_opt8x8.c / kernel_avx512_standard8x8.c (8x8). */
+B2_API int b2_dgemm_kernel(int unroll_m, int unroll_n, long m, long n, long k, double alpha,
+                           const double *sa, const double *sb, double *C, long ldc, void *stream);
+/* FP32 version: the CNAME kernel of sgemm.c:397-412 (16x4). */
+B2_API int b2_sgemm_kernel(int unroll_m, int unroll_n, long m, long n, long k, float alpha,
+                           const float *sa, const float *sb, float *C, long ldc, void *stream);
+/* 3M step: C_cplx (m x n, ldc in complex elements, interleaved re/im) +=
+ * (alphar + i alphai) * A * B with real packed A and B: the CNAME kernels of
+ * zgemm3m_kernel_2x8_skylakex.c:336-351 and cgemm3m_kernel_16x4_skylakex.c:
+ * 415-440. */
+B2_API int b2_zgemm3m_kernel(int unroll_m, int unroll_n, long m, long n, long k, double alphar,
+                             double alphai, const double *sa, const double *sb, double *C,
+                             long ldc, void *stream);
+B2_API int b2_cgemm3m_kernel(int unroll_m, int unroll_n, long m, long n, long k, float alphar,
+                             float alphai, const float *sa, const float *sb, float *C, long ldc,
+                             void *stream);
+/* DTRSM solve kernels dtrsm_solve_{ln,lt,rn,rt}_m*n* (dtrsm_kernel_16x4_skylakex.S:
+ * 1863-2536), contract of dtrsm_kernel_16x4_tester.c:66-199, for any m, n:
+ * side 'L'/'R' and trans 'N'/'T' select ln, lt, rn, rt.  The packed triangle
+ * carries its inverted diagonal; the incoming update is added to C, the
+ * solution is written to C and back into the packed right-hand side (sb for
+ * the left kernels, sa for the right ones). */
+B2_API int b2_dtrsm_kernel(char side, char trans, long m, long n, double *sa, double *sb,
+                           double *C, long ldb, long ldc, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* Grouped GEMM: many independent problems in one persistent launch.  No     */
 /* counterpart API in the reference, whose parallel drivers split one GEMM   */
 /* (src/gemm_driver.c:136-149; OpenBLAS-like_implementation/dgemm.c:449-483   */

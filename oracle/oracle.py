@@ -173,6 +173,34 @@ def ref_gemm3m_kernel(which, m, n, k, alphar, alphai, pa, pb, c):
     lb.kern(m, n, k, alphar, alphai, _ptr(pa), _ptr(pb), _ptr(c), _ld(c))
 
 
+# Reference real GEMM kernels of the OpenBLAS kernel ABI:
+# C(m x n, ldc) += alpha * A_packed * B_packed.  name -> (library, symbol,
+# integer type of m/n/k/ldc, scalar type, A panel width, B panel width).
+GEMM_KERNELS = {
+    "d16x2": ("oblike_dgemm.so", "CNAME", C.c_int, C.c_double, 16, 2),   # dgemm.c:247-263
+    "d4x8": ("dgemm_4x8.so", "kern", C.c_long, C.c_double, 4, 8),        # dgemm_kernel_4x8_skylakex_2.c:661
+    "s16x4": ("oblike_sgemm.so", "CNAME", C.c_int, C.c_float, 16, 4),    # sgemm.c:397-412
+}
+
+
+def panel_widths(unroll: int):
+    """Panel widths a packing of the given unroll produces: full panels, then
+    the remainder in halving widths (the tcopy/ncopy routines, dgemm.c:304-403)."""
+    w, out = unroll, []
+    while w >= 1:
+        out.append(w)
+        w //= 2
+    return out
+
+
+def ref_gemm_kernel(which, m, n, k, alpha, pa, pb, c):
+    """The reference kernel `which` on packed panels, in place on c (Fortran)."""
+    libname, sym, it, st, _, _ = GEMM_KERNELS[which]
+    fn = getattr(ref_lib(libname), sym)
+    fn.argtypes = [it, it, it, st, C.c_void_p, C.c_void_p, C.c_void_p, it]
+    fn(m, n, k, alpha, _ptr(pa), _ptr(pb), _ptr(c), _ld(c))
+
+
 def pack_panels(x: np.ndarray, widths) -> np.ndarray:
     """Greedy panel packing used by the OpenBLAS kernel ABI: rows of x (dim x k)
     cut into panels of the given widths (largest first), each stored k-major."""

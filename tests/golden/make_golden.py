@@ -106,6 +106,46 @@ def gemm3m_kernel_cases(seed):
     return out
 
 
+def gemm_kernel_cases(seed):
+    """Real and 3M kernels of the OpenBLAS kernel ABI on packed panels:
+    C += alpha * A B (real), C_cplx += (ar + i ai) * A B (3M, interleaved C)."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    idx = 0
+    shapes = [(1, 1, 1), (3, 5, 7), (16, 2, 9), (29, 13, 33), (37, 26, 64), (8, 24, 5)]
+    for which in ("d16x2", "d4x8", "s16x4", "c16x4"):
+        if which == "c16x4":
+            um, un, dt = 16, 4, np.float32
+        else:
+            _, _, _, _, um, un = O.GEMM_KERNELS[which]
+            dt = np.float32 if which[0] == "s" else np.float64
+        for (m, n, k) in shapes:
+            a = rng.uniform(-1, 1, (m, k)).astype(dt)
+            b = rng.uniform(-1, 1, (n, k)).astype(dt)
+            pa = O.pack_panels(a, O.panel_widths(um))
+            pb = O.pack_panels(b, O.panel_widths(un))
+            ldc = m + 2
+            if which == "c16x4":
+                c = np.asfortranarray((rng.uniform(-1, 1, (ldc, n)) +
+                                       1j * rng.uniform(-1, 1, (ldc, n))).astype(np.complex64))
+                al = np.array([0.5, -1.5], dt)
+                cout = c.copy(order="F")
+                O.ref_gemm3m_kernel("c16x4", m, n, k, al[0], al[1], pa, pb, cout)
+            else:
+                c = np.asfortranarray(rng.uniform(-1, 1, (ldc, n)).astype(dt))
+                al = np.array([1.25, 0.0], dt)
+                cout = c.copy(order="F")
+                O.ref_gemm_kernel(which, m, n, k, al[0], pa, pb, cout)
+            key = f"g{idx}"
+            out[key + "_meta"] = np.array([m, n, k, um, un], np.int64)
+            out[key + "_kind"] = np.array(which)
+            out[key + "_alpha"] = al
+            out[key + "_a"], out[key + "_b"], out[key + "_c"], out[key + "_out"] = a, b, c, cout
+            idx += 1
+    out["count"] = np.array(idx)
+    return out
+
+
 def main():
     if not (O.ref_available("DGEMM.so") and O.host_has_avx512f()):
         raise SystemExit("reference libraries not built or host lacks AVX-512F")
@@ -113,6 +153,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "sgemm_ref.npz"), **gemm_cases(np.float32, 12))
     np.savez_compressed(os.path.join(HERE, "trsm_kernels_ref.npz"), **trsm_cases(13))
     np.savez_compressed(os.path.join(HERE, "zgemm3m_kernel_ref.npz"), **gemm3m_kernel_cases(14))
+    np.savez_compressed(os.path.join(HERE, "gemm_kernels_ref.npz"), **gemm_kernel_cases(15))
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))
