@@ -77,6 +77,7 @@ def lib() -> C.CDLL:
     L.b2_version.restype = i
     L.b2_set_dgemm_method.argtypes = [i, i]
     L.b2_set_sgemm_method.argtypes = [i]
+    L.b2_set_arg_mode.argtypes = [i]
     gemm_ptrs = [pc, pc, pi, pi, pi, p, p, pi, p, pi, p, p, pi]
     for nm in ("dgemm_", "sgemm_", "SGEMM_", "zgemm3m_", "cgemm3m_"):
         getattr(L, nm).argtypes = gemm_ptrs

@@ -10,6 +10,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "b2_internal.cuh"
@@ -245,10 +246,51 @@ static int pipeline_blocks(int m, int n, int k, size_t elem, int *cols) {
 // block j is copied in (copy-in stream), computed (library stream) and copied
 // out (copy-out stream) while block j+1 is copied in, so the PCIe transfers,
 // which dominate a host-to-host product, overlap the GEMM.
+// Argument-check mode of the real drop-in GEMMs (B2_ARGS_BLAS / _OPENBLAS).
+static std::atomic<int> g_arg_mode{-1};
+static int arg_mode() {
+  int v = g_arg_mode.load();
+  if (v < 0) {
+    const char *e = getenv("B2_ARG_MODE");
+    v = (e && !strcmp(e, "openblas")) ? B2_ARGS_OPENBLAS : B2_ARGS_BLAS;
+    int expect = -1;
+    g_arg_mode.compare_exchange_strong(expect, v);
+    v = g_arg_mode.load();
+  }
+  return v;
+}
+
+// The OpenBLAS-like dgemm_ checks (OpenBLAS-like_implementation/dgemm.c:488-498).
+// Returns true when the call must return now (status already set).
+static bool openblas_arg_checks(char ta, char tb, int m, int n, int k, int lda, int ldb) {
+  if (m < 1 || n < 1) { set_status(B2_OK); return true; }
+  const char *msg = nullptr;
+  int info = 0;
+  if (notrans(ta)) {
+    if (lda < m) msg = "ERROR: LDA < M with column-major matrix A. Please check input parameters.", info = 8;
+  } else if (lda < k) {
+    msg = "ERROR: LDA < K with row-major matrix A. Please check input parameters.", info = 8;
+  }
+  if (!msg) {
+    if (notrans(tb)) {
+      if (ldb < k) msg = "ERROR: LDB < K with column-major matrix B. Please check input parameters.", info = 10;
+    } else if (ldb < n) {
+      msg = "ERROR: LDB < N with row-major matrix B. Please check input parameters.", info = 10;
+    }
+  }
+  if (!msg) return false;
+  printf("%s\n", msg);
+  fflush(stdout);
+  set_status(B2_ERR_ARG, info);
+  return true;
+}
+
 template <typename T, typename F>
 static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *a, int lda,
                        const T *b, int ldb, T beta, T *cm, int ldc, F &&run) {
   int info = 0;
+  if (arg_mode() == B2_ARGS_OPENBLAS && openblas_arg_checks(ta, tb, m, n, k, lda, ldb))
+    return g_status.code;
   int st = check_gemm(ta, tb, m, n, k, lda, ldb, ldc, a, b, cm, &info);
   if (st != B2_OK) { set_status(st, info); return st; }
   if (m == 0 || n == 0) { set_status(B2_OK); return B2_OK; }
@@ -726,6 +768,13 @@ int b2_dgemm_error(char transa, char transb, int m, int n, int k, double alpha,
   }
   set_status(st);
   return st;
+}
+
+int b2_set_arg_mode(int mode) {
+  if (mode != B2_ARGS_BLAS && mode != B2_ARGS_OPENBLAS) return -1;
+  const int prev = arg_mode();
+  g_arg_mode.store(mode);
+  return prev;
 }
 
 int b2_device_error(int clear) {

@@ -70,6 +70,20 @@ B2_API int b2_set_dgemm_method(int method, int slices);
  * env B2_SGEMM_METHOD=fp32|tf32|tf32x3|bf16x3. */
 B2_API int b2_set_sgemm_method(int method);
 
+/* Argument checking of the real drop-in GEMMs (dgemm_, sgemm_, SGEMM_), process-wide:
+ *   B2_ARGS_BLAS (default): BLAS argument positions (xerbla numbering) reported
+ *     through b2_last_error()/b2_last_info(), C untouched;
+ *   B2_ARGS_OPENBLAS: the checks of the reference's OpenBLAS-like dgemm_
+ *     (OpenBLAS-like_implementation/dgemm.c:488-498): M < 1 or N < 1 returns
+ *     silently; LDA / LDB below the rows of A / B print the reference's
+ *     "ERROR: ... Please check input parameters." line on stdout and return.
+ *     LDC < M is still refused (B2_ERR_ARG, info 13): C is staged row by row.
+ * Also settable by env B2_ARG_MODE=blas|openblas.  Returns the previous mode, or
+ * -1 (nothing changed) for an unknown mode. */
+#define B2_ARGS_BLAS 0
+#define B2_ARGS_OPENBLAS 1
+B2_API int b2_set_arg_mode(int mode);
+
 /* ------------------------------------------------------------------------ */
 /* Drop-in Fortran-BLAS symbols                                              */
 /* ------------------------------------------------------------------------ */

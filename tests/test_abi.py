@@ -91,3 +91,39 @@ def test_dtrsm_argument_errors_leave_b_untouched(args, info):
                    kw["lda"], b, kw["ldb"])
     assert ei.value.status == _lib.B2_ERR_ARG and ei.value.info == info
     assert np.array_equal(b, before)
+
+
+def test_openblas_argument_mode(capfd):
+    """B2_ARGS_OPENBLAS: the OpenBLAS-like dgemm_ checks (dgemm.c:488-498) --
+    M < 1 or N < 1 returns silently, a short LDA / LDB prints the reference's
+    message on stdout and returns, C untouched either way."""
+    L = _lib.lib()
+    assert L.b2_set_arg_mode(7) == -1  # unknown mode: nothing changes
+    prev = L.b2_set_arg_mode(1)
+    try:
+        a = np.ones((7, 7), order="F")
+        c = np.full((7, 7), 3.0, order="F")
+        before = c.copy()
+        blas.dgemm("N", "N", -1, 5, 5, 1.0, a, 7, a, 7, 0.0, c, 7)  # silent quick return
+        blas.dgemm("N", "N", 5, 0, 5, 1.0, a, 7, a, 7, 0.0, c, 7)
+        assert np.array_equal(c, before)
+        cases = [("N", "N", 7, 5, 5, 5, 7, "LDA < M with column-major matrix A"),
+                 ("T", "N", 5, 5, 7, 5, 7, "LDA < K with row-major matrix A"),
+                 ("N", "N", 5, 5, 7, 7, 5, "LDB < K with column-major matrix B"),
+                 ("N", "T", 5, 7, 5, 7, 5, "LDB < N with row-major matrix B")]
+        for ta, tb, m, n, k, lda, ldb, text in cases:
+            capfd.readouterr()
+            with pytest.raises(_lib.B2Error) as ei:
+                blas.dgemm(ta, tb, m, n, k, 1.0, a, lda, a, ldb, 0.0, c, 7)
+            assert ei.value.status == _lib.B2_ERR_ARG
+            out = capfd.readouterr().out
+            assert out == f"ERROR: {text}. Please check input parameters.\n", out
+            assert np.array_equal(c, before)
+        af = a.astype(np.float32)
+        cf = c.astype(np.float32)
+        capfd.readouterr()
+        with pytest.raises(_lib.B2Error):
+            blas.sgemm("N", "N", 7, 5, 5, 1.0, af, 5, af, 7, 0.0, cf, 7)
+        assert "LDA < M" in capfd.readouterr().out
+    finally:
+        assert L.b2_set_arg_mode(prev) == 1
