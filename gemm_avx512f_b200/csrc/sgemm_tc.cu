@@ -106,6 +106,59 @@ struct F32Epi {
   }
 };
 
+// Split-K epilogue: the raw FP32 partial of K range ks (the engine's batch
+// index) to W[ks][n][ldw]; sgemm_splitk_reduce_kernel adds the ranges in a
+// fixed order.
+struct F32PartialEpi {
+  float *W;
+  long long plane;
+  int ldw;
+  int M, N;
+  __device__ __forceinline__ void operator()(int ks, int p, int q0, const uint32_t (&v)[32]) const {
+    if (p >= N || q0 >= M) return;
+    float4 *dst = reinterpret_cast<float4 *>(W + ks * plane + (long long)p * ldw + q0);
+#pragma unroll
+    for (int g = 0; g < 8; ++g)
+      dst[g] = make_float4(__uint_as_float(v[4 * g]), __uint_as_float(v[4 * g + 1]),
+                           __uint_as_float(v[4 * g + 2]), __uint_as_float(v[4 * g + 3]));
+  }
+};
+
+// C(m, n) = alpha * sum_ks W[ks][n][m] + beta C (beta != 1 multiplies), the
+// partials summed in FP64 in K order and rounded once.
+__global__ void sgemm_splitk_reduce_kernel(const float *__restrict__ W, long long plane, int ldw,
+                                           int S, int M, int N, float alpha, float beta,
+                                           float *__restrict__ C, int ldc) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  for (int n = blockIdx.y; n < N; n += gridDim.y) {
+    double acc = 0.0;
+    for (int ks = 0; ks < S; ++ks) acc += (double)W[ks * plane + (long long)n * ldw + m];
+    float *c = C + (long long)n * ldc + m;
+    const float a = (float)acc;
+    *c = (beta == 1.f) ? fmaf(alpha, a, *c) : fmaf(alpha, a, beta * *c);
+  }
+}
+
+// K ranges for a product of `tiles` output tiles and `kblocks` K blocks: 1
+// when the tiles already fill the SMs, else the count (at most 16, >= 8 K
+// blocks per range) that best fills whole waves of `sms` CTAs.
+int choose_ksplit(long long tiles, int kblocks, int sms) {
+  if (tiles >= sms) return 1;
+  int best = 1;
+  double best_eff = (double)tiles / sms;
+  for (int S = 2; S <= 16 && S * 8 <= kblocks; ++S) {
+    const long long units = tiles * S;
+    const long long waves = (units + sms - 1) / sms;
+    const double eff = (double)units / (double)(waves * sms);
+    if (eff > best_eff + 0.02) {
+      best_eff = eff;
+      best = S;
+    }
+  }
+  return best;
+}
+
 inline long long round_up(long long x, long long a) { return (x + a - 1) / a * a; }
 
 template <typename T>
@@ -160,12 +213,38 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
   if (rc == B2_OK)
     rc = umma::make_kmajor_map(&tmY, kind, Yp, kt, m, 1, kt * esz, (long long)m * kt * esz, 256);
   if (rc != B2_OK) return rc;
-  F32Epi epi{C, ldc, m, n, alpha, beta};
-  if (bf16)
-    return umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
-                                                  cx->derr, s, "sgemm_umma_bf16");
-  return umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count, cx->derr,
-                                                s, "sgemm_umma_tf32");
+  const long long tiles = ((n + umma::BM - 1) / umma::BM) * (long long)((m + 255) / 256);
+  const int kblocks = (int)((kt * esz + umma::KBLOCK_BYTES - 1) / umma::KBLOCK_BYTES);
+  int S = choose_ksplit(tiles, kblocks, cx->sm_count);
+  if (S > 1) {
+    // the engine may merge ranges; size W for S and pass the count it uses
+    const int kbps = (kblocks + S - 1) / S;
+    S = (kblocks + kbps - 1) / kbps;
+  }
+  if (S == 1) {
+    F32Epi epi{C, ldc, m, n, alpha, beta};
+    if (bf16)
+      return umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
+                                                    cx->derr, s, "sgemm_umma_bf16");
+    return umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
+                                                  cx->derr, s, "sgemm_umma_tf32");
+  }
+  // Split-K: S partial products of K ranges, then one fixed-order reduction.
+  const int ldw = (int)round_up(m, 256);  // whole 256-column tiles stay in bounds
+  const long long plane = (long long)n * ldw;
+  float *W = (float *)workspace(cx, WS_MISC, (size_t)plane * S * sizeof(float));
+  if (!W) return B2_ERR_NOMEM;
+  F32PartialEpi pe{W, plane, ldw, m, n};
+  rc = bf16 ? umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, pe, cx->sm_count,
+                                                     cx->derr, s, "sgemm_umma_bf16", 0, nullptr, S)
+            : umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, pe, cx->sm_count,
+                                                     cx->derr, s, "sgemm_umma_tf32", 0, nullptr, S);
+  if (rc != B2_OK) return rc;
+  dim3 grid((unsigned)((m + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
+  B2_PROF("sgemm_splitk_reduce", s);
+  sgemm_splitk_reduce_kernel<<<grid, 256, 0, s>>>(W, plane, ldw, S, m, n, alpha, beta, C, ldc);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
 }
 
 }  // namespace b2

@@ -195,6 +195,8 @@ __device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[32]) {
 struct Problem {
   int P, Q;        // rows of X and of Y (output tile space P x Q)
   int kblocks;     // K extent in 128-byte blocks
+  int ksplit;      // K ranges per output tile (split-K; 1 = whole K in one accumulator)
+  int kb_per_split;  // K blocks per range (every range is non-empty)
   int nbatch;      // independent products (3-D tensor maps, batch = outer coordinate)
   const int *nbatch_dev;  // if set: the batch count actually run (<= nbatch), read on the device
   int tiles_p, tiles_q;
@@ -248,6 +250,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nbatch = pr.nbatch_dev ? min(*pr.nbatch_dev, pr.nbatch) : pr.nbatch;
   const int total_tiles = pr.tiles_p * pr.tiles_q * nbatch;
+  // work units: (tile, K range) pairs, the K range innermost
+  const int total_units = total_tiles * pr.ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -286,10 +290,12 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t phase = 0;
       long issued = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x) {
+      for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x) {
+        const int t = u / pr.ksplit, ks = u - t * pr.ksplit;
         int b, tp, tq;
         tile_coords(pr, t, b, tp, tq);
-        for (int kb = 0; kb < pr.kblocks; ++kb) {
+        const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, pr.derr)) { ok = false; break; }
           const uint32_t sx = base + stage * L::STAGE_BYTES;
           const uint32_t sy = sx + L::X_BYTES;
@@ -321,13 +327,15 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t phase = 0;
       int it = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < total_tiles && ok; t += gridDim.x, ++it) {
+      for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++it) {
+        const int ks = u % pr.ksplit;
+        const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
         const int acc = it & 1;
         const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
         if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag, pr.derr)) { ok = false; break; }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-        for (int kb = 0; kb < pr.kblocks; ++kb) {
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait(full_bar(stage), phase, abort_flag, pr.derr)) { ok = false; break; }
           tc_fence_after();
           const uint32_t sx = base + stage * L::STAGE_BYTES;
@@ -335,7 +343,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
           for (int kk = 0; kk < KBLOCK_BYTES / 32; ++kk) {
             tc_mma<KIND>(d_tmem, sw128_desc(sx + kk * 32), sw128_desc(sy + kk * 32), idesc,
-                         (kb | kk) ? 1u : 0u);
+                         (kb != kb0 || kk) ? 1u : 0u);
           }
           tc_commit(empty_bar(stage));  // frees the stage once these MMAs have read it
           if (++stage == STAGES) { stage = 0; phase ^= 1u; }
@@ -353,7 +361,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     // ---------------------------------------------------------- epilogue
     const int quarter = warp & 3;  // TMEM lanes this warp may access
     int it = 0;
-    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, ++it) {
+    for (int u = blockIdx.x; u < total_units; u += gridDim.x, ++it) {
+      const int t = u / pr.ksplit, ks = u - t * pr.ksplit;
       int b, tp, tq;
       tile_coords(pr, t, b, tp, tq);
       const int acc = it & 1;
@@ -367,7 +376,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint32_t v[32];
         tmem_ld32(taddr + (uint32_t)(c * 32), v);
         tmem_ld_wait(v);
-        epi(b, p, tq * BN + c * 32, v);
+        epi(b * pr.ksplit + ks, p, tq * BN + c * 32, v);  // batch x K range
       }
       tc_fence_before();
       __syncwarp();
@@ -687,7 +696,8 @@ int make_kmajor_map(CUtensorMap *map, int kind, const void *base, long long kele
 template <int KIND, int BN, int STAGES, class Epi>
 int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
            int nbatch, const Epi &epi, int sm_count, int *derr, cudaStream_t s,
-           const char *prof_name, int max_ctas = 0, const int *nbatch_dev = nullptr) {
+           const char *prof_name, int max_ctas = 0, const int *nbatch_dev = nullptr,
+           int ksplit = 1) {
   using L = SmemLayout<BN, STAGES>;
   Problem pr;
   pr.P = P;
@@ -699,7 +709,14 @@ int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long lo
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;
   pr.derr = derr;
-  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch;
+  // split-K: ranges of ceil(kblocks / ksplit) blocks, their count recomputed so
+  // that none is empty (an empty range would leave its accumulator unwritten)
+  if (ksplit < 1) ksplit = 1;
+  if (ksplit > pr.kblocks) ksplit = pr.kblocks > 0 ? pr.kblocks : 1;
+  pr.kb_per_split = (pr.kblocks + ksplit - 1) / ksplit;
+  pr.ksplit = pr.kb_per_split > 0 ? (pr.kblocks + pr.kb_per_split - 1) / pr.kb_per_split : 1;
+  if (pr.ksplit < 1) pr.ksplit = 1;
+  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch * pr.ksplit;
   if (total <= 0) return B2_OK;
   int grid = (int)(total < sm_count ? total : sm_count);
   if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
@@ -727,6 +744,8 @@ int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, lo
   pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
   pr.nbatch = nbatch;
   pr.nbatch_dev = nbatch_dev;
+  pr.ksplit = 1;
+  pr.kb_per_split = pr.kblocks;
   pr.tiles_p = (P + PAIR_BM - 1) / PAIR_BM;
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;

@@ -35,8 +35,9 @@ def _run(dev, meth, ta, tb, m, n, k, alpha, a, b, beta, c):
 
 @pytest.mark.parametrize("meth", METHODS)
 @pytest.mark.parametrize("m,n,k", [(1, 1, 1), (37, 53, 29), (129, 65, 385), (300, 257, 1000),
-                                   (1024, 1024, 1024)])
+                                   (1024, 1024, 1024), (2048, 160, 1536)])
 def test_parity_with_reference_sgemm(cuda, meth, m, n, k):
+    # shapes with fewer output tiles than SMs run split-K (partials + reduction)
     rng = np.random.default_rng(m * 3 + k)
     for ta, tb in [("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")]:
         a = np.asfortranarray(rng.uniform(-1, 1, (m, k) if ta == "N" else (k, m)).astype(np.float32))
