@@ -1,4 +1,8 @@
-// gemm3m.cu -- complex GEMM by the 3M method in ONE fused launch.
+// gemm3m.cu -- complex GEMM by the 3M method.
+//
+// Products below 2^24 multiply-adds run in ONE fused launch (below); larger
+// ones run the three real products as the library's own GEMMs between a
+// pre-add pass and a combine pass (gemm3m_three_gemms, at the end).
 //
 // Replaces the OpenBLAS gemm3m driver + the reference's 3M kernels
 // (zgemm3m_kernel_2x8_skylakex.c:336-351, zgemm3m_kernel_8x4_skylakex.c:309-334,
@@ -250,6 +254,85 @@ __global__ void cscale_kernel(int M, int N, T br, T bi, T *__restrict__ C, int l
 
 }  // namespace
 
+// ------------------------------------------ large products: 3 real GEMMs --
+// Real and imaginary parts of op(X) (R x Cc, element (r, c) at
+// X[2*(r*ld + c)] when transposed, else X[2*(c*ld + r)]; imaginary part times
+// sgn for conjugation) and their sum, column-major with leading dimension R.
+template <typename T>
+__global__ void prep3m_kernel(const T *__restrict__ X, int ld, bool trans, T sgn, int R, int Cc,
+                              T *__restrict__ outr, T *__restrict__ outi, T *__restrict__ outs) {
+  const long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= R) return;
+  for (long long c = blockIdx.y; c < Cc; c += gridDim.y) {
+    const T *p = X + 2 * (trans ? r * ld + c : c * ld + r);
+    const T re = p[0], im = sgn * p[1];
+    const long long o = r + c * (long long)R;
+    outr[o] = re;
+    outi[o] = im;
+    outs[o] = re + im;
+  }
+}
+
+// C = alpha (P1 - P2 + i (P3 - P1 - P2)) + beta C, beta applied when != 1.
+template <typename T>
+__global__ void combine3m_kernel(const T *__restrict__ P, long long plane, int M, int N, T ar,
+                                 T ai, T br, T bi, T *__restrict__ C, int ldc) {
+  const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (m >= M) return;
+  for (long long n = blockIdx.y; n < N; n += gridDim.y) {
+    const long long o = m + n * M;
+    const T p1 = P[o], p2 = P[plane + o], p3 = P[2 * plane + o];
+    epilogue3m(C, ldc, (int)m, (int)n, p1, p2, p3, ar, ai, br, bi);
+  }
+}
+
+// Products of at least 2^24 multiply-adds: the three real products run as
+// the library's own GEMMs (FP64 DMMA for zgemm3m; 3xTF32 tensor-core SGEMM,
+// FP32-class accuracy, for cgemm3m) between one pre-add pass and one
+// post-combination pass -- both HBM-bound -- instead of the fused tile kernel,
+// whose in-register pre-adds cap it below the plain GEMMs' rate.
+template <typename T>
+int gemm3m_three_gemms(char ta, char tb, int m, int n, int k, T ar, T ai, T br, T bi,
+                       const T *A, int lda, const T *B, int ldb, T *C, int ldc, cudaStream_t s) {
+  Ctx *cx = ctx();
+  if (!cx) return B2_ERR_NO_DEVICE;
+  const bool tA = !(ta == 'N' || ta == 'n' || ta == 'R' || ta == 'r');
+  const bool tB = !(tb == 'N' || tb == 'n' || tb == 'R' || tb == 'r');
+  const T sA = (ta == 'C' || ta == 'c' || ta == 'R' || ta == 'r') ? (T)-1 : (T)1;
+  const T sB = (tb == 'C' || tb == 'c' || tb == 'R' || tb == 'r') ? (T)-1 : (T)1;
+  const long long pa = (long long)m * k, pb = (long long)k * n, pc = (long long)m * n;
+  T *W = (T *)workspace(cx, WS_3M, (size_t)(3 * pa + 3 * pb + 3 * pc) * sizeof(T));
+  if (!W) return B2_ERR_NOMEM;
+  T *Ar = W, *Ai = Ar + pa, *As = Ai + pa;
+  T *Br = As + pa, *Bi = Br + pb, *Bs = Bi + pb;
+  T *P = Bs + pb;
+  {
+    B2_PROF("gemm3m_prep", s);
+    dim3 ga((unsigned)((m + 255) / 256), (unsigned)(k < 4096 ? k : 4096));
+    prep3m_kernel<T><<<ga, 256, 0, s>>>(A, lda, tA, sA, m, k, Ar, Ai, As);
+    dim3 gb((unsigned)((k + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
+    prep3m_kernel<T><<<gb, 256, 0, s>>>(B, ldb, tB, sB, k, n, Br, Bi, Bs);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
+  // beta = 0 still multiplies the output (reference semantics): start at zero
+  B2_CUDA_TRY(cudaMemsetAsync(P, 0, (size_t)(3 * pc) * sizeof(T), s));
+  const T *X[3] = {Ar, Ai, As}, *Y[3] = {Br, Bi, Bs};
+  for (int t = 0; t < 3; ++t) {
+    int st;
+    if constexpr (sizeof(T) == 8)
+      st = dgemm_fp64('N', 'N', m, n, k, 1.0, X[t], m, Y[t], k, 0.0, P + t * pc, m, s, nullptr);
+    else
+      st = sgemm_dispatch('N', 'N', m, n, k, 1.0f, X[t], m, Y[t], k, 0.0f, P + t * pc, m,
+                          B2_METHOD_TF32X3, s);
+    if (st != B2_OK) return st;
+  }
+  B2_PROF("gemm3m_combine", s);
+  dim3 gc((unsigned)((m + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
+  combine3m_kernel<T><<<gc, 256, 0, s>>>(P, pc, m, n, ar, ai, br, bi, C, ldc);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
 template <typename T>
 int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T *A, int lda,
                   const T *B, int ldb, const T *beta, T *C, int ldc, cudaStream_t s) {
@@ -264,6 +347,8 @@ int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T
     B2_CUDA_TRY(cudaGetLastError());
     return B2_OK;
   }
+  if ((double)m * n * k >= 16777216.0)
+    return gemm3m_three_gemms<T>(ta, tb, m, n, k, ar, ai, br, bi, A, lda, B, ldb, C, ldc, s);
   dim3 grid((m + G_BM - 1) / G_BM, (n + G_BN - 1) / G_BN);
   const int smem = (int)(12 * G_BK * G_LD * sizeof(T));
   if constexpr (sizeof(T) == 8) {

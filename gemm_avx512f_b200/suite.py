@@ -22,7 +22,8 @@ workloads:
   grouped  4096 problems, M, N, K log-uniform in [16, 1024] (seed 3), half
            FP32 half FP64, random transposes: one grouped launch, its CUDA
            graph plan, and one call per problem.
-  complex  zgemm3m / cgemm3m, M=N=K=2048, real and imaginary parts U[-1,1).
+  complex  zgemm3m / cgemm3m, M=N=K=2048, real and imaginary parts U[-1,1): three
+           real GEMMs (FP64 DMMA / 3xTF32) between pre-add and combine passes.
   trsm     DTRSM L/L/N/N, n=16384, 4096 right-hand sides (seed 4), diagonal
            n + U[0,1): FP64 and Ozaki trailing updates, scaled residual.
   select   learned configuration selector on the committed timing database:
@@ -268,9 +269,9 @@ def run_complex(ctx, out, quick):
         if name == "zgemm3m":
             rec.update(bound="fp64 tensor (nominal), 6n^3 issued", peak=P["fp64_tflops"],
                        frac=6.0 * n ** 3 / ms / 1e9 / P["fp64_tflops"])
-        else:
-            rec.update(bound="fp32 SIMT (nominal), 6n^3 issued", peak=P["fp32_tflops"],
-                       frac=6.0 * n ** 3 / ms / 1e9 / P["fp32_tflops"])
+        else:  # three 3xTF32 tensor-core products: 3 MMAs per issued product
+            rec.update(bound="tf32 tensor, 3 MMAs per product, 6n^3 issued",
+                       peak=P["tf32_tflops"], frac=3 * 6.0 * n ** 3 / ms / 1e9 / P["tf32_tflops"])
         emit(out, rec)
 
 
