@@ -40,11 +40,20 @@ struct GroupDesc {
   long long tile_offset;
 };
 
-// Stage a GT_K-deep panel: op(A) tile (64 x 16) and op(B) tile (16 x 64) into
-// shared memory as As[k][m] and Bs[k][n] (stride GT_LD), zero outside.
+// A GT_K-deep panel: op(A) tile (64 x 16) and op(B) tile (16 x 64), 4
+// elements of each per thread.  load_panel fetches it from global memory into
+// registers (zero outside the problem), store_panel writes it to shared
+// memory as As[k][m] and Bs[k][n] (stride GT_LD).  Tiles double-buffer the
+// panels: the next panel's loads are in flight while the current one is
+// multiplied.
 template <typename T>
-__device__ __forceinline__ void stage_panel(const GroupDesc &g, int m0, int n0, int k0, T *As,
-                                            T *Bs) {
+struct PanelRegs {
+  T a[4], b[4];
+};
+
+template <typename T>
+__device__ __forceinline__ void load_panel(const GroupDesc &g, int m0, int n0, int k0,
+                                           PanelRegs<T> &r) {
   const T *A = (const T *)g.A;
   const T *B = (const T *)g.B;
 #pragma unroll
@@ -53,22 +62,61 @@ __device__ __forceinline__ void stage_panel(const GroupDesc &g, int m0, int n0, 
     int mm, kk;
     if (g.ta) { kk = idx % GT_K; mm = idx / GT_K; } else { mm = idx % GT_M; kk = idx / GT_M; }
     const int gm = m0 + mm, gk = k0 + kk;
-    T v = 0;
-    if (gm < g.m && gk < g.k)
-      v = g.ta ? A[(long long)gm * g.lda + gk] : A[(long long)gk * g.lda + gm];
-    As[kk * GT_LD + mm] = v;
+    r.a[e] = (gm < g.m && gk < g.k)
+                 ? (g.ta ? A[(long long)gm * g.lda + gk] : A[(long long)gk * g.lda + gm])
+                 : (T)0;
     int nn;
     if (g.tb) { nn = idx % GT_N; kk = idx / GT_N; } else { kk = idx % GT_K; nn = idx / GT_K; }
     const int gn = n0 + nn, gk2 = k0 + kk;
-    T w = 0;
-    if (gn < g.n && gk2 < g.k)
-      w = g.tb ? B[(long long)gk2 * g.ldb + gn] : B[(long long)gn * g.ldb + gk2];
-    Bs[kk * GT_LD + nn] = w;
+    r.b[e] = (gn < g.n && gk2 < g.k)
+                 ? (g.tb ? B[(long long)gk2 * g.ldb + gn] : B[(long long)gn * g.ldb + gk2])
+                 : (T)0;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void store_panel(const GroupDesc &g, const PanelRegs<T> &r, T *As,
+                                            T *Bs) {
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int idx = threadIdx.x + 256 * e;
+    int mm, kk;
+    if (g.ta) { kk = idx % GT_K; mm = idx / GT_K; } else { mm = idx % GT_M; kk = idx / GT_M; }
+    As[kk * GT_LD + mm] = r.a[e];
+    int nn;
+    if (g.tb) { nn = idx % GT_N; kk = idx / GT_N; } else { kk = idx % GT_K; nn = idx / GT_K; }
+    Bs[kk * GT_LD + nn] = r.b[e];
+  }
+}
+
+constexpr int GT_PANEL = GT_K * GT_LD;  // elements of one operand panel
+constexpr int GT_STAGE = 2 * GT_PANEL;  // A and B panels of one stage
+
+// Runs the K loop of one tile over two shared-memory stages; `mac(As, Bs)`
+// multiplies one resident panel pair.
+template <typename T, class Mac>
+__device__ __forceinline__ void tile_k_loop(const GroupDesc &g, int m0, int n0, T *buf, Mac mac) {
+  const int nk = (g.k + GT_K - 1) / GT_K;
+  PanelRegs<T> r;
+  if (nk > 0) {
+    load_panel<T>(g, m0, n0, 0, r);
+    store_panel<T>(g, r, buf, buf + GT_PANEL);
+  }
+  __syncthreads();
+  for (int it = 0; it < nk; ++it) {
+    T *As = buf + (it & 1) * GT_STAGE;
+    const bool more = it + 1 < nk;
+    if (more) load_panel<T>(g, m0, n0, (it + 1) * GT_K, r);
+    mac(As, As + GT_PANEL);
+    if (more) {
+      T *An = buf + ((it + 1) & 1) * GT_STAGE;
+      store_panel<T>(g, r, An, An + GT_PANEL);
+    }
+    __syncthreads();  // the stage just read is refilled two iterations later
   }
 }
 
 __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
-  double *As = sm, *Bs = sm + GT_K * GT_LD;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gq = lane >> 2, t = lane & 3;
   const int wm0 = (warp >> 2) * 32, wn0 = (warp & 3) * 16;
@@ -79,10 +127,7 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
-  for (int k0 = 0; k0 < g.k; k0 += GT_K) {
-    __syncthreads();
-    stage_panel<double>(g, m0, n0, k0, As, Bs);
-    __syncthreads();
+  tile_k_loop<double>(g, m0, n0, sm, [&](const double *As, const double *Bs) {
 #pragma unroll
     for (int kk = 0; kk < GT_K; kk += 4) {
       double af[2][2], bf[2];
@@ -102,7 +147,7 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
               : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
               : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
     }
-  }
+  });
   double *C = (double *)g.C;
   const bool one = (g.beta == 1.0);
 #pragma unroll
@@ -121,17 +166,13 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
 }
 
 __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
-  float *As = sm, *Bs = sm + GT_K * GT_LD;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   float acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
-  for (int k0 = 0; k0 < g.k; k0 += GT_K) {
-    __syncthreads();
-    stage_panel<float>(g, m0, n0, k0, As, Bs);
-    __syncthreads();
+  tile_k_loop<float>(g, m0, n0, sm, [&](const float *As, const float *Bs) {
 #pragma unroll
     for (int kk = 0; kk < GT_K; ++kk) {
       const float4 a = *reinterpret_cast<const float4 *>(&As[kk * GT_LD + tx * 4]);
@@ -142,7 +183,7 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
-  }
+  });
   float *C = (float *)g.C;
   const float al = (float)g.alpha, be = (float)g.beta;
   const bool one = (be == 1.f);
@@ -161,7 +202,7 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
 __global__ void __launch_bounds__(256)
     grouped_kernel(const GroupDesc *__restrict__ d, int count, long long total_tiles,
                    unsigned long long *counter) {
-  __shared__ __align__(16) double sm[2 * GT_K * GT_LD];
+  __shared__ __align__(16) double sm[2 * GT_STAGE];  // two stages of A and B panels
   __shared__ long long tile_s;
   for (;;) {
     __syncthreads();
