@@ -81,17 +81,64 @@ def physical_cores() -> int:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (read-only queries)."""
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    Read-only NVML queries every 10 ms from a background thread (so even a
+    sub-second timed region gets dozens of samples); nvidia-smi -lms 200 when
+    NVML cannot be loaded."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.samples = []
+        self.max_mhz = None
+        self.stop_flag = False
+
+    def _nvml_handle(self):
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08X:%02X:%02X.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def poll():
+                while not self.stop_flag:
+                    try:
+                        mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h) \
+                            if hasattr(nv, "nvmlDeviceGetCurrentClocksEventReasons") \
+                            else nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                        self.samples.append((float(mhz), int(rs)))
+                    except Exception:
+                        pass
+                    time.sleep(0.01)
+
+            import threading
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -101,6 +148,16 @@ class Clocks:
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag = True
+            self.thread.join(timeout=2)
+            if not self.samples:
+                return None
+            reasons = sorted({nm for _, rs in self.samples for nm, bit in self.BITS.items()
+                              if rs & bit})
+            return {"sm_mhz": statistics.median(m for m, _ in self.samples),
+                    "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(self.samples), "source": "nvml 10 ms"}
         if self.proc is None:
             return None
         time.sleep(0.3)
@@ -127,7 +184,7 @@ class Clocks:
         if not sms:
             return None
         return {"sm_mhz": statistics.median(sms), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sms)}
+                "samples": len(sms), "source": "nvidia-smi 200 ms"}
 
 
 # ------------------------------------------------------------ CPU legs ----
@@ -396,9 +453,10 @@ def e2e_leg(args, L, a_h, b_h, method):
     dt = (time.perf_counter() - t0) / steps
     L.b2_set_dgemm_method(_lib_fp64(), 0)
     return {"value": 2.0 * n ** 3 / dt / 1e12, "unit": "TFLOPS",
-            "h2d_bytes_per_step": 3 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
+            "h2d_bytes_per_step": 2 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
             "ms_per_step": dt * 1e3,
-            "note": "drop-in dgemm_ on pinned host A, B, C (C is read: beta==0 keeps NaN)"}
+            "note": "drop-in dgemm_ on pinned host A, B, C: A and B copied in, C copied out; "
+                    "with beta == 0 C is scanned on the host (all finite, so not copied in)"}
 
 
 def _lib_fp64():

@@ -46,11 +46,14 @@ def test_dgemm_dropin_host_parity(cuda, m, n, k, ta, tb):
         assert e <= TOL, (m, n, k, ta, tb, al, be, e)
 
 
-@pytest.mark.parametrize("method", ["fp64", "ozaki"])
-def test_dgemm_dropin_pipelined_host_operands(cuda, method):
+@pytest.mark.parametrize("method,plant_nan", [("fp64", True), ("ozaki", True), ("fp64", False),
+                                              ("ozaki", False)])
+def test_dgemm_dropin_pipelined_host_operands(cuda, method, plant_nan):
     """Host operands of a product >= 2^32 flops go through the column-block
     copy/compute/copy pipeline; blocks of 256-multiples leave a ragged last
-    block here (n = 1800), and op(B) blocks are row blocks of B for 'T'."""
+    block here (n = 1800), and op(B) blocks are row blocks of B for 'T'.
+    beta == 0 with an all-finite C skips copying C in (the device blocks are
+    zeroed); a NaN in C makes the library copy it, and the NaN survives."""
     m, n, k = 1000, 1800, 1300
     rng = np.random.default_rng(77)
     u = np.finfo(np.float64).eps / 2
@@ -58,16 +61,17 @@ def test_dgemm_dropin_pipelined_host_operands(cuda, method):
     try:
         for ta, tb in [("N", "N"), ("T", "T")]:
             a, b, c, ar, br = _case(rng, np.float64, m, n, k, ta, tb)
-            c[5, 1700] = np.nan  # beta == 0 still multiplies C: NaN survives, as in the reference
+            if plant_nan:
+                c[5, 1700] = np.nan  # beta == 0 still multiplies C: NaN survives, as in the reference
             ref = c.copy(order="F")
             O.gemm(ta, tb, m, n, k, 1.25, a[:ar], b[:br], 0.0, ref[:m])
             got = c.copy(order="F")
             blas.dgemm(ta, tb, m, n, k, 1.25, a, a.shape[0], b, b.shape[0], 0.0, got,
                        got.shape[0])
             assert np.array_equal(got[m:], c[m:]), "padding rows of C were written"
-            assert np.isnan(got[5, 1700]) and np.isnan(ref[5, 1700])
+            assert np.isnan(got[5, 1700]) == plant_nan and np.isnan(ref[5, 1700]) == plant_nan
             fin = np.isfinite(ref[:m])
-            assert fin.sum() == m * n - 1
+            assert fin.sum() == m * n - (1 if plant_nan else 0)
             g, r = np.where(fin, got[:m], 0.0), np.where(fin, ref[:m], 0.0)
             e = normalized(g, r, k, a[:ar], b[:br], u)
             assert e <= TOL, (method, ta, tb, e)
