@@ -221,6 +221,22 @@ def cpu_dgemm_rate(a: np.ndarray, b: np.ndarray, n: int, seconds: float):
                       f"{dt:.1f} s"}
 
 
+def max_over_ranks(ms: float, dist, device=None) -> float:
+    """The slowest rank's time: every rank passes its own device-timed ms and
+    gets the maximum (the job is as slow as its slowest replica)."""
+    import torch
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_tflops(world: int, flops_per_step: float, steps: int, ms: float) -> float:
+    """Whole-job rate: every replica ran `steps` products of `flops_per_step`
+    (weak scaling) in `ms`, the max over ranks."""
+    return world * flops_per_step * steps / (ms / 1e3) / 1e12
+
+
 def reference_arm(args, rank: int):
     if rank != 0:
         return None
@@ -309,11 +325,9 @@ def gpu_arm(args, rank: int, world: int):
     ck = clocks.stop()
     ms = e0.elapsed_time(e1)
     if dist:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, dev)
     ms_step = ms / args.steps
-    value = world * flops * args.steps / (ms / 1e3) / 1e12
+    value = job_tflops(world, flops, args.steps, ms)
 
     # ---- dominant kernel roofline (live CUDA-event durations over the timed region)
     peaks, peak_src = load_peaks()
