@@ -401,7 +401,7 @@ def gpu_arm(args, rank: int, world: int):
 
     # ---- end to end through the drop-in dgemm_ with pinned host buffers
     if not args.no_e2e:
-        out["e2e"] = e2e_leg(args, L, a_h, b_h, method)
+        out["e2e"] = e2e_leg(args, L, a_h, b_h, method, dist, dev, world)
 
     # ---- CPU baseline (reference on the host cores), rank 0 at N=1 only
     if not args.no_cpu and rank == 0 and world == 1:
@@ -442,7 +442,7 @@ def profile_traffic(kname: str):
     return None
 
 
-def e2e_leg(args, L, a_h, b_h, method):
+def e2e_leg(args, L, a_h, b_h, method, dist=None, dev=None, world=1):
     import torch
 
     n = args.n
@@ -461,12 +461,16 @@ def e2e_leg(args, L, a_h, b_h, method):
 
     call()
     steps = max(2, min(args.steps, 5))
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
-        call()
+        call()  # synchronous: C is back in host memory when it returns
     dt = (time.perf_counter() - t0) / steps
+    if dist:  # the job is as slow as its slowest replica; count every replica's work
+        dt = max_over_ranks(dt * 1e3, dist, dev) / 1e3
     L.b2_set_dgemm_method(_lib_fp64(), 0)
-    return {"value": 2.0 * n ** 3 / dt / 1e12, "unit": "TFLOPS",
+    return {"value": world * 2.0 * n ** 3 / dt / 1e12, "unit": "TFLOPS",
             "h2d_bytes_per_step": 2 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
             "ms_per_step": dt * 1e3,
             "note": "drop-in dgemm_ on pinned host A, B, C: A and B copied in, C copied out; "
