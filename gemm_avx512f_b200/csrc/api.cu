@@ -391,7 +391,9 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
         if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[j], c->h2d);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->ev_in[j], 0);
         if (e != cudaSuccess) break;
+        ozaki_pipeline_block(j);
         st = run((const T *)da, dla, (const T *)bd, dlb, cd, dlc, nj, s);
+        ozaki_pipeline_block(-1);
         if (st != B2_OK) break;
         e = cudaEventRecord(c->ev_done[j], s);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->d2h, c->ev_done[j], 0);

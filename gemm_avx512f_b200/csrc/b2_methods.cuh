@@ -36,6 +36,9 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                 cudaStream_t s);
 int ozaki_auto_moduli(int k);
 void ozaki_set_variant(int v);  // INT8 engine shape of the allocating path (0..4; -1 = default)
+// Column block j of the host-operand pipeline on this thread (-1 = none): lets
+// the Ozaki DGEMM reuse A's exponents and slices across the blocks.
+void ozaki_pipeline_block(int j);
 
 // SGEMM methods (sgemm.cu).
 int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,

@@ -745,6 +745,22 @@ int default_oz_variant() {
 }
 thread_local int g_oz_variant = default_oz_variant();
 
+// Column block of the host-operand pipeline this thread is running (-1:
+// none).  The pipeline calls the Ozaki DGEMM once per block of B and C with
+// the same A; blocks after the first reuse A's exponents and residue slices,
+// and an automatic count is fixed at 16 moduli for the whole pipeline (the
+// per-block choice cannot change A's slices once they are cut; the extra
+// modulus is hidden under the copies that bound the pipeline).
+thread_local int g_pipe_block = -1;
+struct ASideCache {
+  bool valid = false;
+  const double *A = nullptr;
+  int m = 0, k = 0, lda = 0, s = 0, H = 0;
+  bool tA = false;
+  const void *Y = nullptr, *sc = nullptr;
+};
+thread_local ASideCache g_aside;
+
 int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, int n, int m, int s,
                 long long kp, long long planeX, long long planeY, const ResidueEpi &epi,
                 int device, int sm_count, int *derr, cudaStream_t st, const int *s_dev) {
@@ -836,6 +852,11 @@ size_t norm_scratch_bytes(int R, int K) {
 
 }  // namespace
 
+void ozaki_pipeline_block(int j) {
+  g_pipe_block = j;
+  if (j < 0) g_aside.valid = false;
+}
+
 void ozaki_set_variant(int v) {
   g_oz_variant = (v >= 0 && v < OZ_VARIANTS) ? v : default_oz_variant();
 }
@@ -858,6 +879,7 @@ int ozaki_auto_moduli(int k) {
 // (uniform data: about -0.4; a = u exp(g): about -1.9; a = u exp(4g): about -10).
 constexpr double OZ_LOG2_RHO_MIN = -4.0;
 
+
 int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
                 const double *B, int ldb, double beta, double *C, int ldc, int slices,
                 cudaStream_t st) {
@@ -867,8 +889,14 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   if (k <= 0 || alpha == 0.0) return beta == 1.0 ? B2_OK : scale_matrix_d(m, n, beta, C, ldc, st);
   // slices <= 0: automatic count, s_base or (heavy-tailed inputs) s_base + 1,
   // chosen on the device after the norm pass; buffers are sized for s_max.
-  const bool adaptive = slices <= 0;
-  const int s_base = adaptive ? ozaki_auto_moduli(k) : slices;
+  const bool piped = g_pipe_block >= 0;
+  bool adaptive = slices <= 0;
+  int s_base = adaptive ? ozaki_auto_moduli(k) : slices;
+  if (piped && adaptive) {  // fixed count across the pipeline's blocks
+    adaptive = false;
+    s_base = s_base < OZ_MAX ? s_base + 1 : OZ_MAX;
+  }
+  if (!piped) g_aside.valid = false;
   if (s_base < 2 || s_base > OZ_MAX) return B2_ERR_ARG;
   const int s_max = adaptive && s_base < OZ_MAX ? s_base + 1 : s_base;
   int rc = upload_tables(cx->device, st);
@@ -907,8 +935,15 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   void *scrA = sc + o_scr;
   void *scrB = (uint8_t *)scrA + round_up(nsA, 256);
 
+  // Blocks after the first of a pipeline reuse A's exponents (sigA) and
+  // residue slices (Y) when they are still in place for the same A.
+  const bool reuse_a = piped && g_pipe_block > 0 && kchunks == 1 && g_aside.valid &&
+                       g_aside.A == A && g_aside.m == m && g_aside.k == k && g_aside.lda == lda &&
+                       g_aside.tA == tA && g_aside.s == s_base && g_aside.H == t.H &&
+                       g_aside.Y == (const void *)Y && g_aside.sc == (const void *)sc;
   if (adaptive) B2_CUDA_TRY(cudaMemsetAsync(stat, 0, 4 * sizeof(double), st));
-  rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
+  if (!reuse_a)
+    rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
   if (rc == B2_OK)
     rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, scrB, adaptive ? stat + 2 : nullptr, st);
   if (rc != B2_OK) return rc;
@@ -922,7 +957,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
 
   for (int c = 0; c < kchunks && rc == B2_OK; ++c) {
     const int kc0 = c * KCH, kcl = (k - kc0 < KCH) ? k - kc0 : KCH;
-    {
+    if (!reuse_a) {
       dim3 grid((kcl + 63) / 64, (m + 31) / 32);
       B2_PROF(asr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
       if (asr == 1)
@@ -960,6 +995,18 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   int *plan_word = (int *)((uint8_t *)cx->pinned + 64);
   B2_CUDA_TRY(cudaMemcpyAsync(plan_word, s_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
   B2_CUDA_TRY(cudaEventRecord(cx->plan_ev, st));
+  if (piped && kchunks == 1 && !reuse_a) {
+    g_aside.valid = true;
+    g_aside.A = A;
+    g_aside.m = m;
+    g_aside.k = k;
+    g_aside.lda = lda;
+    g_aside.tA = tA;
+    g_aside.s = s_base;
+    g_aside.H = t.H;
+    g_aside.Y = Y;
+    g_aside.sc = sc;
+  }
   g_last_plan.s = s_base;
   g_last_plan.kchunks = kchunks;
   g_last_plan.word = plan_word;
