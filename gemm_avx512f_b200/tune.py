@@ -148,7 +148,11 @@ def main(argv=None) -> int:
     ap.add_argument("--out", default=os.path.join(os.path.dirname(__file__), "data"))
     ap.add_argument("--db", default=None, help="reuse a timing database instead of sweeping")
     ap.add_argument("--select", action="store_true",
-                    help="pick epochs/lr on a validation split of the training shapes")
+                    help="pick clip/epochs/lr/seed on a validation split of the training shapes")
+    ap.add_argument("--clips", default="none,1.5,1.0", help="validation grid: target clips")
+    ap.add_argument("--epochs-grid", default="600,1000", help="validation grid: epochs")
+    ap.add_argument("--lrs", default="1e-3,3e-3", help="validation grid: learning rates")
+    ap.add_argument("--seeds", default="", help="validation grid: training seeds (default: one)")
     args = ap.parse_args(argv)
     os.makedirs(args.out, exist_ok=True)
     key = gpu_key()
@@ -178,22 +182,26 @@ def main(argv=None) -> int:
 
     ok = allowed_mask()
     trials = []
-    epochs, lr, clip = args.epochs, args.lr, None
+    epochs, lr, clip, tseed = args.epochs, args.lr, None, args.seed + 4
     if args.select:
         nv = ntr // 10
-        for cl in (None, 1.5, 1.0):
+        clips = [None if c == "none" else float(c) for c in args.clips.split(",")]
+        seeds = [int(v) for v in args.seeds.split(",")] if args.seeds else [args.seed + 4]
+        for cl in clips:
             Tt = targets(cl)
-            for ep in (600, 1000):
-                for lrc in (1e-3, 3e-3):
-                    wv, _ = train(X[:ntr - nv], Tt[:ntr - nv], ep, lrc, args.seed + 4)
-                    pv = predict(wv, X[ntr - nv:ntr])
-                    rv = regret(ms[ntr - nv:ntr], np.where(ok[None, :], pv, np.inf).argmin(1))
-                    trials.append({"clip": cl, "epochs": ep, "lr": lrc,
-                                   "val_regret_mean": float(rv.mean())})
+            for ep in (int(v) for v in args.epochs_grid.split(",")):
+                for lrc in (float(v) for v in args.lrs.split(",")):
+                    for sd in seeds:
+                        wv, _ = train(X[:ntr - nv], Tt[:ntr - nv], ep, lrc, sd)
+                        pv = predict(wv, X[ntr - nv:ntr])
+                        rv = regret(ms[ntr - nv:ntr],
+                                    np.where(ok[None, :], pv, np.inf).argmin(1))
+                        trials.append({"clip": cl, "epochs": ep, "lr": lrc, "seed": sd,
+                                       "val_regret_mean": float(rv.mean())})
         best = min(trials, key=lambda t: t["val_regret_mean"])
-        epochs, lr, clip = best["epochs"], best["lr"], best["clip"]
+        epochs, lr, clip, tseed = best["epochs"], best["lr"], best["clip"], best["seed"]
     t0 = time.time()
-    w, loss = train(X[:ntr], targets(clip)[:ntr], epochs, lr, args.seed + 4)
+    w, loss = train(X[:ntr], targets(clip)[:ntr], epochs, lr, tseed)
     t_train = time.time() - t0
     pred = predict(w, X[ntr:])
     choice = np.where(ok[None, :], pred, np.inf).argmin(1)
@@ -205,7 +213,7 @@ def main(argv=None) -> int:
                             log2ms=T.astype(np.float16), train=ntr)
     report = {"gpu": key, "shapes": len(shapes), "train": ntr, "heldout": args.heldout,
               "configs": NCFG, "sweep_seconds": t_sweep, "train_seconds": t_train,
-              "epochs": epochs, "lr": lr, "validation_trials": trials,
+              "epochs": epochs, "lr": lr, "seed": tseed, "validation_trials": trials,
               "target": "log2(ms / fastest allowed ms) per shape", "clip": clip,
               "final_train_mse_log2": loss, "regret_mlp": summarize(r_mlp),
               "regret_heuristic": summarize(r_heur),
