@@ -29,6 +29,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "b2_internal.cuh"
 #include "b2_profile.cuh"
 
@@ -764,9 +766,9 @@ int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, lo
   cfg.stream = s;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  static int resident_pairs[64] = {0};  // per device, filled on first use
+  static std::atomic<int> resident_pairs[64];  // per device, filled on first use (0 = unknown)
   const int dslot = device >= 0 && device < 64 ? device : 0;
-  if (resident_pairs[dslot] == 0) {
+  if (resident_pairs[dslot].load() == 0) {
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
     if (e != cudaSuccess) return cuda_fail(e, "umma pair smem attribute");
@@ -777,13 +779,14 @@ int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, lo
       (void)cudaGetLastError();
       return e != cudaSuccess ? cuda_fail(e, "umma pair occupancy") : (int)B2_ERR_UNSUPPORTED;
     }
-    resident_pairs[dslot] = nc;
+    resident_pairs[dslot].store(nc);
   } else {
     cudaError_t e =
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
     if (e != cudaSuccess) return cuda_fail(e, "umma pair smem attribute");
   }
-  const int pairs = (int)(total < resident_pairs[dslot] ? total : resident_pairs[dslot]);
+  const int resident = resident_pairs[dslot].load();
+  const int pairs = (int)(total < resident ? total : resident);
   cfg.gridDim = dim3(2 * pairs);
   B2_PROF(prof_name, s);
   cudaError_t e = cudaLaunchKernelEx(&cfg, kern, tmX, tmY, pr, epi);
