@@ -470,38 +470,62 @@ def e2e_leg(args, L, a_h, b_h, method, dist=None, dev=None, world=1):
     if dist:  # the job is as slow as its slowest replica; count every replica's work
         dt = max_over_ranks(dt * 1e3, dist, dev) / 1e3
     L.b2_set_dgemm_method(_lib_fp64(), 0)
-    # the copy-in bound: these bytes at this box's pinned host-to-device rate
-    h2d_bytes = 2 * 8 * n * n
-    h2d_gbs = pinned_h2d_gbs(pa, dev)
-    bound_ms = h2d_bytes / (h2d_gbs * 1e9) * 1e3 if h2d_gbs else None
+    # the copy bound: these bytes at this box's pinned copy rates -- copy-in
+    # alone, and copy-in plus copy-out run at the same time (the pipeline's
+    # steady state)
+    h2d_bytes, d2h_bytes = 2 * 8 * n * n, 8 * n * n
+    h2d_gbs, duplex_gbs = pinned_copy_gbs(pa, pc, dev)
+    bound_ms = None
+    if h2d_gbs and duplex_gbs:
+        bound_ms = max(h2d_bytes / (h2d_gbs * 1e9), (h2d_bytes + d2h_bytes) / (duplex_gbs * 1e9)) * 1e3
     return {"value": world * 2.0 * n ** 3 / dt / 1e12, "unit": "TFLOPS",
-            "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": 8 * n * n,
-            "ms_per_step": dt * 1e3, "pcie_h2d_gbs": h2d_gbs, "copy_in_bound_ms": bound_ms,
-            "frac_of_copy_in_bound": (bound_ms / (dt * 1e3)) if bound_ms else None,
+            "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
+            "ms_per_step": dt * 1e3, "pcie_h2d_gbs": h2d_gbs,
+            "pcie_h2d_plus_d2h_gbs": duplex_gbs, "copy_bound_ms": bound_ms,
+            "frac_of_copy_bound": (bound_ms / (dt * 1e3)) if bound_ms else None,
             "note": "drop-in dgemm_ on pinned host A, B, C: A and B copied in, C copied out; "
                     "with beta == 0 C is scanned on the host (all finite, so not copied in)"}
 
 
-def pinned_h2d_gbs(pinned, dev):
-    """Pinned host-to-device copy rate (GB/s) of this box: one 512 MiB copy,
-    best of 3, CUDA events."""
+def pinned_copy_gbs(pin_src, pin_dst, dev):
+    """This box's pinned copy rates (GB/s): host-to-device alone, and
+    host-to-device plus device-to-host on two streams at once (bytes of both
+    directions per second).  512 MiB per direction, best of 3, CUDA events."""
     import torch
 
     try:
-        src = pinned[: 64 * 1024 * 1024]
-        dst = torch.empty(src.numel(), dtype=src.dtype, device=dev)
-        best = None
+        nel = min(64 * 1024 * 1024, pin_src.numel(), pin_dst.numel())
+        src, hdst = pin_src[:nel], pin_dst[:nel]
+        d_in = torch.empty(nel, dtype=src.dtype, device=dev)
+        d_out = torch.zeros(nel, dtype=src.dtype, device=dev)
+        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        nbytes = nel * src.element_size()
+        best_in = best_both = None
         for _ in range(3):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            dst.copy_(src, non_blocking=True)
-            e1.record()
+            with torch.cuda.stream(s_in):
+                e0.record()
+                d_in.copy_(src, non_blocking=True)
+                e1.record()
             torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1)
-            best = ms if best is None else min(best, ms)
-        return src.numel() * src.element_size() / (best / 1e3) / 1e9
+            t = e0.elapsed_time(e1)
+            best_in = t if best_in is None else min(best_in, t)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s_in):
+                e0.record()
+                d_in.copy_(src, non_blocking=True)
+            s_out.wait_event(e0)
+            with torch.cuda.stream(s_out):
+                hdst.copy_(d_out, non_blocking=True)
+            s_in.wait_stream(s_out)
+            with torch.cuda.stream(s_in):
+                e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            best_both = t if best_both is None else min(best_both, t)
+        return nbytes / (best_in / 1e3) / 1e9, 2 * nbytes / (best_both / 1e3) / 1e9
     except Exception:
-        return None
+        return None, None
 
 
 def _lib_fp64():

@@ -47,9 +47,10 @@ struct CtxOwner {
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->h2d) cudaStreamSynchronize(c->h2d), cudaStreamDestroy(c->h2d);
     if (c->d2h) cudaStreamSynchronize(c->d2h), cudaStreamDestroy(c->d2h);
-    for (int i = 0; i < Ctx::PIPE_MAX; ++i) {
+    for (int i = 0; i < Ctx::PIPE_EVENTS; ++i) {
       if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
       if (c->ev_done[i]) cudaEventDestroy(c->ev_done[i]);
+      if (c->ev_c[i]) cudaEventDestroy(c->ev_c[i]);
     }
     if (c->plan_ev) cudaEventDestroy(c->plan_ev);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -95,9 +96,10 @@ Ctx *ctx() {
     delete c;
     return nullptr;
   }
-  for (int i = 0; i < Ctx::PIPE_MAX; ++i) {
+  for (int i = 0; i < Ctx::PIPE_EVENTS; ++i) {
     if (cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_c[i], cudaEventDisableTiming) != cudaSuccess) {
       (void)cudaGetLastError();
       delete c;
       return nullptr;
@@ -275,8 +277,8 @@ static int pipeline_blocks(int m, int n, int k, size_t elem, int *cols) {
 }
 
 // Shared host-or-device driver for the real drop-in GEMMs.  run(A, lda, B,
-// ldb, C, ldc, ncols, stream) computes columns [0, ncols) of C from the B
-// columns it is given.  Host operands of a large product go through a
+// ldb, C, ldc, mrows, ncols, stream) computes the mrows x ncols block of C
+// from the op(A) rows and B columns it is given.  Host operands of a large product go through a
 // three-stream pipeline over column blocks of B and C: A is copied once, then
 // block j is copied in (copy-in stream), computed (library stream) and copied
 // out (copy-out stream) while block j+1 is copied in, so the PCIe transfers,
@@ -335,7 +337,7 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
   const bool need_ab = (k > 0 && alpha != (T)0);
   const bool dev = is_device_ptr(cm) && (!need_ab || (is_device_ptr(a) && is_device_ptr(b)));
   if (dev) {
-    st = run(a, lda, b, ldb, cm, ldc, n, s);
+    st = run(a, lda, b, ldb, cm, ldc, m, n, s);
   } else {
     const int ra = notrans(ta) ? m : k, ca = notrans(ta) ? k : m;
     const int rb = notrans(tb) ? k : n, cb = notrans(tb) ? n : k;
@@ -350,7 +352,7 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
         if (st == B2_OK) st = stage_in(c, WS_STAGE_B, b, rb, cb, ldb, sizeof(T), &db, &dlb, s);
       }
       if (st == B2_OK) st = stage_in(c, WS_STAGE_C, cm, m, n, ldc, sizeof(T), &dc, &dlc, s);
-      if (st == B2_OK) st = run((const T *)da, dla, (const T *)db, dlb, (T *)dc, dlc, n, s);
+      if (st == B2_OK) st = run((const T *)da, dla, (const T *)db, dlb, (T *)dc, dlc, m, n, s);
       if (st == B2_OK) st = stage_out(cm, ldc, dc, dlc, m, n, sizeof(T), s);
     } else {
       // Full-size device copies (no buffer is reused, so no block waits for
@@ -364,42 +366,107 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
       dc = workspace(c, WS_STAGE_C, (size_t)dlc * n * sizeof(T));
       if (!da || !db || !dc) st = B2_ERR_NOMEM;
       cudaError_t e = cudaSuccess;
-      if (st == B2_OK)
-        e = cudaMemcpy2DAsync(da, (size_t)dla * sizeof(T), a, (size_t)lda * sizeof(T),
-                              (size_t)ra * sizeof(T), ca, cudaMemcpyDefault, c->h2d);
-      // beta == 0 reads C only to keep a NaN or Inf already there (0 * C);
-      // when a host scan (overlapping A's copy) finds C all finite, its device
-      // blocks are zeroed instead of copied -- a quarter of the PCIe bytes.
-      const bool c_in = !(beta == (T)0 && st == B2_OK && e == cudaSuccess &&
-                          !is_device_ptr(cm) && host_all_finite(cm, m, n, ldc));
+      // Rows [r0, r1) of op(A): rows of A for 'N', columns of A for 'T'.
+      auto copy_a_rows = [&](int r0, int r1) {
+        return notrans(ta)
+                   ? cudaMemcpy2DAsync((T *)da + r0, (size_t)dla * sizeof(T), a + r0,
+                                       (size_t)lda * sizeof(T), (size_t)(r1 - r0) * sizeof(T),
+                                       ca, cudaMemcpyDefault, c->h2d)
+                   : cudaMemcpy2DAsync((T *)da + (size_t)r0 * dla, (size_t)dla * sizeof(T),
+                                       a + (size_t)r0 * lda, (size_t)lda * sizeof(T),
+                                       (size_t)k * sizeof(T), r1 - r0, cudaMemcpyDefault, c->h2d);
+      };
+      auto a_rows = [&](int r0) {
+        return notrans(ta) ? (const T *)da + r0 : (const T *)da + (size_t)r0 * dla;
+      };
+      // Block 0 is computed in two row halves: the first half starts as soon as
+      // the top rows of A are in, so C starts flowing back while the rest of A
+      // is still being copied (the copy-out would otherwise start only after
+      // all of A and one block of B had arrived).
+      const int mh = m >= 512 ? (m / 2) / 256 * 256 : 0;
+      const bool split0 = mh > 0 && mh < m;
+      auto block_cols = [&](int j, int *j0, int *nj) {
+        *j0 = j * cw;
+        *nj = (n - *j0 < cw) ? n - *j0 : cw;
+      };
+      auto b_dev = [&](int j0) {
+        return notrans(tb) ? (T *)db + (size_t)j0 * dlb : (T *)db + j0;
+      };
+      // beta == 0 reads C only to keep a NaN or Inf already there (0 * C):
+      // then the host scans C while the copies run, and an all-finite C is
+      // zeroed on the device instead of copied in (a quarter of the PCIe
+      // bytes).  Any other beta needs C, copied with its block of B.
+      const bool scan_c = beta == (T)0 && !is_device_ptr(cm);
+      auto copy_c_in = [&](int j0, int nj) {
+        return cudaMemcpy2DAsync((T *)dc + (size_t)j0 * dlc, (size_t)dlc * sizeof(T),
+                                 cm + (size_t)j0 * ldc, (size_t)ldc * sizeof(T),
+                                 (size_t)m * sizeof(T), nj, cudaMemcpyDefault, c->h2d);
+      };
+      // 1. Queue the copies on the copy-in stream: A's top rows, block 0 of B
+      //    (and of C), A's other rows, then the other blocks; ev_in[j] marks
+      //    block j (and all of A queued before it) in device memory,
+      //    ev_in[PIPE_MAX] the rest of A.
+      if (st == B2_OK) e = copy_a_rows(0, split0 ? mh : m);
+      for (int j = 0; j < nb && st == B2_OK && e == cudaSuccess; ++j) {
+        int j0, nj;
+        block_cols(j, &j0, &nj);
+        const T *bh = notrans(tb) ? b + (size_t)j0 * ldb : b + j0;
+        e = notrans(tb)
+                ? cudaMemcpy2DAsync(b_dev(j0), (size_t)dlb * sizeof(T), bh, (size_t)ldb * sizeof(T),
+                                    (size_t)k * sizeof(T), nj, cudaMemcpyDefault, c->h2d)
+                : cudaMemcpy2DAsync(b_dev(j0), (size_t)dlb * sizeof(T), bh, (size_t)ldb * sizeof(T),
+                                    (size_t)nj * sizeof(T), k, cudaMemcpyDefault, c->h2d);
+        if (e == cudaSuccess && !scan_c) e = copy_c_in(j0, nj);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[j], c->h2d);
+        if (j == 0 && split0 && e == cudaSuccess) {
+          e = copy_a_rows(mh, m);
+          if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[Ctx::PIPE_MAX], c->h2d);
+        }
+      }
+      // 2. The scan (beta == 0), overlapping the copies queued above.  A C
+      //    holding a NaN or Inf is then copied in after them (rare: the
+      //    blocks wait for all of B).
+      const bool zero_c = scan_c && st == B2_OK && e == cudaSuccess &&
+                          host_all_finite(cm, m, n, ldc);
+      // 3. Per block: C in place, compute once its copies are in, copy C out.
       int issued = 0;
       for (int j = 0; j < nb && st == B2_OK && e == cudaSuccess; ++j) {
-        const int j0 = j * cw, nj = (n - j0 < cw) ? n - j0 : cw;
-        const T *bh = notrans(tb) ? b + (size_t)j0 * ldb : b + j0;
-        T *bd = notrans(tb) ? (T *)db + (size_t)j0 * dlb : (T *)db + j0;
-        e = notrans(tb)
-                ? cudaMemcpy2DAsync(bd, (size_t)dlb * sizeof(T), bh, (size_t)ldb * sizeof(T),
-                                    (size_t)k * sizeof(T), nj, cudaMemcpyDefault, c->h2d)
-                : cudaMemcpy2DAsync(bd, (size_t)dlb * sizeof(T), bh, (size_t)ldb * sizeof(T),
-                                    (size_t)nj * sizeof(T), k, cudaMemcpyDefault, c->h2d);
+        int j0, nj;
+        block_cols(j, &j0, &nj);
+        const T *bd = b_dev(j0);
         T *cd = (T *)dc + (size_t)j0 * dlc;
         T *ch = cm + (size_t)j0 * ldc;
-        if (e == cudaSuccess)
-          e = c_in ? cudaMemcpy2DAsync(cd, (size_t)dlc * sizeof(T), ch, (size_t)ldc * sizeof(T),
-                                       (size_t)m * sizeof(T), nj, cudaMemcpyDefault, c->h2d)
-                   : cudaMemsetAsync(cd, 0, (size_t)dlc * nj * sizeof(T), c->h2d);
-        if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[j], c->h2d);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->ev_in[j], 0);
+        if (zero_c) {
+          e = cudaMemsetAsync(cd, 0, (size_t)dlc * nj * sizeof(T), s);
+        } else if (scan_c) {
+          e = copy_c_in(j0, nj);
+          if (e == cudaSuccess) e = cudaEventRecord(c->ev_c[j], c->h2d);
+          if (e == cudaSuccess) e = cudaStreamWaitEvent(s, c->ev_c[j], 0);
+        }
+        // rows [r0, r1) of block j once copy-in event `ev` has fired
+        auto part = [&](int ev, int done, int r0, int r1) {
+          cudaError_t pe = cudaStreamWaitEvent(s, c->ev_in[ev], 0);
+          if (pe != cudaSuccess) return pe;
+          ozaki_pipeline_block(j);
+          st = run(a_rows(r0), dla, bd, dlb, cd + r0, dlc, r1 - r0, nj, s);
+          ozaki_pipeline_block(-1);
+          if (st != B2_OK) return cudaSuccess;
+          pe = cudaEventRecord(c->ev_done[done], s);
+          if (pe == cudaSuccess) pe = cudaStreamWaitEvent(c->d2h, c->ev_done[done], 0);
+          if (pe == cudaSuccess)
+            pe = cudaMemcpy2DAsync(ch + r0, (size_t)ldc * sizeof(T), cd + r0,
+                                   (size_t)dlc * sizeof(T), (size_t)(r1 - r0) * sizeof(T), nj,
+                                   cudaMemcpyDefault, c->d2h);
+          return pe;
+        };
         if (e != cudaSuccess) break;
-        ozaki_pipeline_block(j);
-        st = run((const T *)da, dla, (const T *)bd, dlb, cd, dlc, nj, s);
-        ozaki_pipeline_block(-1);
+        if (j == 0 && split0) {
+          e = part(0, 0, 0, mh);
+          if (e == cudaSuccess && st == B2_OK) e = part(Ctx::PIPE_MAX, Ctx::PIPE_MAX, mh, m);
+        } else {
+          e = part(j, j, 0, m);
+        }
         if (st != B2_OK) break;
-        e = cudaEventRecord(c->ev_done[j], s);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->d2h, c->ev_done[j], 0);
-        if (e == cudaSuccess)
-          e = cudaMemcpy2DAsync(ch, (size_t)ldc * sizeof(T), cd, (size_t)dlc * sizeof(T),
-                                (size_t)m * sizeof(T), nj, cudaMemcpyDefault, c->d2h);
         ++issued;
       }
       if (st == B2_OK && e != cudaSuccess) st = cuda_fail(e, "pipelined staging");
@@ -581,8 +648,8 @@ void dgemm_(const char *transa, const char *transb, const int *m, const int *n, 
   const double al = *alpha, be = *beta;
   gemm_dropin<double>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
                       [&](const double *A, int la, const double *B, int lb, double *C, int lc,
-                          int ncols, cudaStream_t s) {
-                        return dgemm_device(ta, tb, *m, ncols, *k, al, A, la, B, lb, be, C, lc,
+                          int mrows, int ncols, cudaStream_t s) {
+                        return dgemm_device(ta, tb, mrows, ncols, *k, al, A, la, B, lb, be, C, lc,
                                             B2_METHOD_DEFAULT, 0, s);
                       });
 }
@@ -598,8 +665,8 @@ void sgemm_(const char *transa, const char *transb, const int *m, const int *n, 
   const float al = *alpha, be = *beta;
   gemm_dropin<float>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
                      [&](const float *A, int la, const float *B, int lb, float *C, int lc,
-                         int ncols, cudaStream_t s) {
-                       return sgemm_device(ta, tb, *m, ncols, *k, al, A, la, B, lb, be, C, lc,
+                         int mrows, int ncols, cudaStream_t s) {
+                       return sgemm_device(ta, tb, mrows, ncols, *k, al, A, la, B, lb, be, C, lc,
                                            B2_METHOD_DEFAULT, s);
                      });
 }

@@ -52,8 +52,9 @@ struct Ctx {
   // Host-operand pipeline of the drop-in GEMMs: copy-in and copy-out streams
   // and one (copied-in, computed) event pair per column block.
   static constexpr int PIPE_MAX = 32;
+  static constexpr int PIPE_EVENTS = PIPE_MAX + 1;  // + the second row half of block 0
   cudaStream_t h2d = nullptr, d2h = nullptr;
-  cudaEvent_t ev_in[PIPE_MAX] = {}, ev_done[PIPE_MAX] = {};
+  cudaEvent_t ev_in[PIPE_EVENTS] = {}, ev_done[PIPE_EVENTS] = {}, ev_c[PIPE_EVENTS] = {};
   cudaEvent_t plan_ev = nullptr;  // marks the copy-back of the last Ozaki modulus count
 };
 
