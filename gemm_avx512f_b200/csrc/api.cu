@@ -423,12 +423,13 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
           if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[Ctx::PIPE_MAX], c->h2d);
         }
       }
-      // 2. The scan (beta == 0), overlapping the copies queued above.  A C
-      //    holding a NaN or Inf is then copied in after them (rare: the
-      //    blocks wait for all of B).
-      const bool zero_c = scan_c && st == B2_OK && e == cudaSuccess &&
-                          host_all_finite(cm, m, n, ldc);
-      // 3. Per block: C in place, compute once its copies are in, copy C out.
+      // 2. Per block, while the copies queued above run: with beta == 0 the
+      //    host scans the block's C (an all-finite block is zeroed on the
+      //    device; one holding a NaN or Inf is copied in after everything
+      //    queued, which is rare), then the block is computed once its copies
+      //    are in and its C copied out.  Scanning block by block lets block 0
+      //    start before the scan of all of C has finished.
+      if (sizeof(T) == 8) ozaki_pipeline_rows(-1, nullptr, 0, 0);
       int issued = 0;
       for (int j = 0; j < nb && st == B2_OK && e == cudaSuccess; ++j) {
         int j0, nj;
@@ -436,7 +437,7 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
         const T *bd = b_dev(j0);
         T *cd = (T *)dc + (size_t)j0 * dlc;
         T *ch = cm + (size_t)j0 * ldc;
-        if (zero_c) {
+        if (scan_c && host_all_finite(ch, m, nj, ldc)) {
           e = cudaMemsetAsync(cd, 0, (size_t)dlc * nj * sizeof(T), s);
         } else if (scan_c) {
           e = copy_c_in(j0, nj);
@@ -447,9 +448,8 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
         auto part = [&](int ev, int done, int r0, int r1) {
           cudaError_t pe = cudaStreamWaitEvent(s, c->ev_in[ev], 0);
           if (pe != cudaSuccess) return pe;
-          ozaki_pipeline_block(j);
+          if (sizeof(T) == 8) ozaki_pipeline_rows(j, (const double *)da, m, r0);
           st = run(a_rows(r0), dla, bd, dlb, cd + r0, dlc, r1 - r0, nj, s);
-          ozaki_pipeline_block(-1);
           if (st != B2_OK) return cudaSuccess;
           pe = cudaEventRecord(c->ev_done[done], s);
           if (pe == cudaSuccess) pe = cudaStreamWaitEvent(c->d2h, c->ev_done[done], 0);
@@ -469,6 +469,7 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
         if (st != B2_OK) break;
         ++issued;
       }
+      if (sizeof(T) == 8) ozaki_pipeline_rows(-1, nullptr, 0, 0);
       if (st == B2_OK && e != cudaSuccess) st = cuda_fail(e, "pipelined staging");
       // Every stream drains before returning, whatever failed.
       cudaError_t e1 = cudaStreamSynchronize(c->h2d);

@@ -36,9 +36,12 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                 cudaStream_t s);
 int ozaki_auto_moduli(int k);
 void ozaki_set_variant(int v);  // INT8 engine shape of the allocating path (0..4; -1 = default)
-// Column block j of the host-operand pipeline on this thread (-1 = none): lets
-// the Ozaki DGEMM reuse A's exponents and slices across the blocks.
-void ozaki_pipeline_block(int j);
+// Host-operand pipeline state of this thread: the next Ozaki DGEMM computes
+// rows [r0, r0 + m) of op(A) for column block j, op(A) being m_full rows whose
+// row 0 is at a_full (device).  A's exponents and residue slices are kept for
+// all m_full rows and reused by later blocks.  j < 0 ends the pipeline and
+// drops what was kept.
+void ozaki_pipeline_rows(int j, const double *a_full, int m_full, int r0);
 
 // SGEMM methods (sgemm.cu).
 int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,

@@ -746,18 +746,46 @@ int default_oz_variant() {
 thread_local int g_oz_variant = default_oz_variant();
 
 // Column block of the host-operand pipeline this thread is running (-1:
-// none).  The pipeline calls the Ozaki DGEMM once per block of B and C with
-// the same A; blocks after the first reuse A's exponents and residue slices,
-// and an automatic count is fixed at 16 moduli for the whole pipeline (the
-// per-block choice cannot change A's slices once they are cut; the extra
-// modulus is hidden under the copies that bound the pipeline).
-thread_local int g_pipe_block = -1;
+// none) and the rows of op(A) the next call computes.  The pipeline calls the
+// Ozaki DGEMM once per block of B and C (block 0 in two row halves, the first
+// starting before all of A has arrived) with the same A; each row range of A
+// is cut into exponents and residue slices once, and an automatic count is
+// fixed at 16 moduli for the whole pipeline (the per-block choice cannot
+// change A's slices once they are cut; the extra modulus is hidden under the
+// copies that bound the pipeline).
+struct PipeRows {
+  int block = -1;
+  const double *a_full = nullptr;
+  int m_full = 0, r0 = 0;
+};
+thread_local PipeRows g_pipe;
+// A's exponents (sigA) and slices (Y) for the pipeline's whole op(A), with the
+// row ranges already cut (at most 8 disjoint ranges, merged when they touch).
 struct ASideCache {
   bool valid = false;
   const double *A = nullptr;
   int m = 0, k = 0, lda = 0, s = 0, H = 0;
   bool tA = false;
   const void *Y = nullptr, *sc = nullptr;
+  int nr = 0;
+  int lo[8], hi[8];
+  bool covers(int r0, int r1) const {
+    for (int i = 0; i < nr; ++i)
+      if (lo[i] <= r0 && r1 <= hi[i]) return true;
+    return false;
+  }
+  void add(int r0, int r1) {
+    for (int i = 0; i < nr;) {  // absorb every range that overlaps or touches
+      if (lo[i] <= r1 && r0 <= hi[i]) {
+        r0 = lo[i] < r0 ? lo[i] : r0;
+        r1 = hi[i] > r1 ? hi[i] : r1;
+        lo[i] = lo[nr - 1], hi[i] = hi[nr - 1], --nr;
+      } else {
+        ++i;
+      }
+    }
+    if (nr < 8) lo[nr] = r0, hi[nr] = r1, ++nr;
+  }
 };
 thread_local ASideCache g_aside;
 
@@ -852,8 +880,11 @@ size_t norm_scratch_bytes(int R, int K) {
 
 }  // namespace
 
-void ozaki_pipeline_block(int j) {
-  g_pipe_block = j;
+void ozaki_pipeline_rows(int j, const double *a_full, int m_full, int r0) {
+  g_pipe.block = j;
+  g_pipe.a_full = j < 0 ? nullptr : a_full;
+  g_pipe.m_full = j < 0 ? 0 : m_full;
+  g_pipe.r0 = j < 0 ? 0 : r0;
   if (j < 0) g_aside.valid = false;
 }
 
@@ -889,7 +920,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   if (k <= 0 || alpha == 0.0) return beta == 1.0 ? B2_OK : scale_matrix_d(m, n, beta, C, ldc, st);
   // slices <= 0: automatic count, s_base or (heavy-tailed inputs) s_base + 1,
   // chosen on the device after the norm pass; buffers are sized for s_max.
-  const bool piped = g_pipe_block >= 0;
+  const bool piped = g_pipe.block >= 0;
   bool adaptive = slices <= 0;
   int s_base = adaptive ? ozaki_auto_moduli(k) : slices;
   if (piped && adaptive) {  // fixed count across the pipeline's blocks
@@ -915,32 +946,42 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   const int kchunks = (k + KCH - 1) / KCH;
   const long long kp = round_up(k < KCH ? k : KCH, 16);
   const long long mp = round_up(m, 16);
-  const long long planeY = (long long)m * kp, planeX = (long long)n * kp;
+  // Inside the pipeline, this call's rows [r0, r0 + m) of op(A) are a view
+  // of the pipeline's whole op(A) (m_all rows): A's exponents and slices live
+  // at their place in full-size arrays, so every block can reuse them.
+  const bool rows_view = piped && kchunks == 1 && g_pipe.a_full && g_pipe.r0 >= 0 &&
+                         g_pipe.r0 + m <= g_pipe.m_full &&
+                         g_pipe.a_full + (long long)g_pipe.r0 * asr == A;
+  if (!rows_view) g_aside.valid = false;
+  const int m_all = rows_view ? g_pipe.m_full : m, r0 = rows_view ? g_pipe.r0 : 0;
+  const long long planeY = (long long)m_all * kp, planeX = (long long)n * kp;
   const long long planeR = (long long)n * mp;
 
-  int8_t *Y = (int8_t *)workspace(cx, WS_OZ_Y, (size_t)planeY * s_max);
+  int8_t *Yall = (int8_t *)workspace(cx, WS_OZ_Y, (size_t)planeY * s_max);
   int8_t *X = (int8_t *)workspace(cx, WS_OZ_X, (size_t)planeX * s_max);
   uint8_t *Rb = (uint8_t *)workspace(cx, WS_OZ_R, (size_t)planeR * s_max);
   const size_t nsA = norm_scratch_bytes(m, k), nsB = norm_scratch_bytes(n, k);
-  // [sigma|tau][stat A (2 doubles), stat B (2 doubles), modulus count][norm A][norm B]
-  const size_t o_stat = round_up((m + n) * sizeof(int), 256);
+  // [sigma (m_all)|tau][stat A (2 doubles), stat B (2 doubles), modulus count][norm A][norm B]
+  const size_t o_stat = round_up((m_all + n) * sizeof(int), 256);
   const size_t o_scr = o_stat + 256;
   const size_t sc_bytes = o_scr + round_up(nsA, 256) + nsB + 512;
   uint8_t *sc = (uint8_t *)workspace(cx, WS_OZ_SCALE, sc_bytes);
-  if (!Y || !X || !Rb || !sc) return B2_ERR_NOMEM;
-  int *sigA = (int *)sc;
-  int *tauB = sigA + m;
+  if (!Yall || !X || !Rb || !sc) return B2_ERR_NOMEM;
+  int *sigA = (int *)sc + r0;
+  int *tauB = (int *)sc + m_all;
+  int8_t *Y = Yall + (long long)r0 * kp;
   double *stat = (double *)(sc + o_stat);
   int *s_dev = (int *)(stat + 4);
   void *scrA = sc + o_scr;
   void *scrB = (uint8_t *)scrA + round_up(nsA, 256);
 
-  // Blocks after the first of a pipeline reuse A's exponents (sigA) and
-  // residue slices (Y) when they are still in place for the same A.
-  const bool reuse_a = piped && g_pipe_block > 0 && kchunks == 1 && g_aside.valid &&
-                       g_aside.A == A && g_aside.m == m && g_aside.k == k && g_aside.lda == lda &&
-                       g_aside.tA == tA && g_aside.s == s_base && g_aside.H == t.H &&
-                       g_aside.Y == (const void *)Y && g_aside.sc == (const void *)sc;
+  // A pipeline block reuses A's exponents (sigA) and residue slices (Y) when
+  // its rows were already cut for the same A and are still in place.
+  const bool same_a = rows_view && g_aside.valid && g_aside.A == g_pipe.a_full &&
+                      g_aside.m == m_all && g_aside.k == k && g_aside.lda == lda &&
+                      g_aside.tA == tA && g_aside.s == s_base && g_aside.H == t.H &&
+                      g_aside.Y == (const void *)Yall && g_aside.sc == (const void *)sc;
+  const bool reuse_a = same_a && g_aside.covers(r0, r0 + m);
   if (adaptive) B2_CUDA_TRY(cudaMemsetAsync(stat, 0, 4 * sizeof(double), st));
   if (!reuse_a)
     rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
@@ -995,17 +1036,21 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   int *plan_word = (int *)((uint8_t *)cx->pinned + 64);
   B2_CUDA_TRY(cudaMemcpyAsync(plan_word, s_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
   B2_CUDA_TRY(cudaEventRecord(cx->plan_ev, st));
-  if (piped && kchunks == 1 && !reuse_a) {
-    g_aside.valid = true;
-    g_aside.A = A;
-    g_aside.m = m;
-    g_aside.k = k;
-    g_aside.lda = lda;
-    g_aside.tA = tA;
-    g_aside.s = s_base;
-    g_aside.H = t.H;
-    g_aside.Y = Y;
-    g_aside.sc = sc;
+  if (rows_view && !reuse_a) {
+    if (!same_a) {
+      g_aside.valid = true;
+      g_aside.A = g_pipe.a_full;
+      g_aside.m = m_all;
+      g_aside.k = k;
+      g_aside.lda = lda;
+      g_aside.tA = tA;
+      g_aside.s = s_base;
+      g_aside.H = t.H;
+      g_aside.Y = Yall;
+      g_aside.sc = sc;
+      g_aside.nr = 0;
+    }
+    g_aside.add(r0, r0 + m);
   }
   g_last_plan.s = s_base;
   g_last_plan.kchunks = kchunks;
