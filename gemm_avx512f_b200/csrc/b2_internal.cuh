@@ -45,6 +45,7 @@ struct Ctx {
   size_t ws_bytes[WS_COUNT] = {};
   int *derr = nullptr;        // device error word
   void *pinned = nullptr;     // small pinned scratch for host reads
+  void *pinned_dev = nullptr; // its device address (kernels store to it directly), or null
   int dgemm_method = B2_METHOD_FP64;
   int dgemm_slices = 0;
   int sgemm_method = B2_METHOD_FP32;
@@ -52,10 +53,10 @@ struct Ctx {
   // Host-operand pipeline of the drop-in GEMMs: copy-in and copy-out streams
   // and one (copied-in, computed) event pair per column block.
   static constexpr int PIPE_MAX = 32;
-  static constexpr int PIPE_EVENTS = PIPE_MAX + 1;  // + the second row half of block 0
+  static constexpr int PIPE_EVENTS = PIPE_MAX + 2;  // + the second row halves of the first and last blocks
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_in[PIPE_EVENTS] = {}, ev_done[PIPE_EVENTS] = {}, ev_c[PIPE_EVENTS] = {};
-  cudaEvent_t plan_ev = nullptr;  // marks the copy-back of the last Ozaki modulus count
+  cudaEvent_t plan_ev = nullptr;  // marks the host store of the last Ozaki modulus count
 };
 
 Ctx *ctx();                          // initialises on first use; nullptr if no device

@@ -345,7 +345,8 @@ __global__ void norm_finalize_kernel(const double *__restrict__ pmax,
 // block.
 __global__ void ozaki_decide_kernel(const double *statA, const double *statB, int adaptive,
                                     int s_base, int s_hi, int dH, double log2_rho_min,
-                                    int *s_dev, int *sigA, int m, int *tauB, int n) {
+                                    int *s_dev, int *sigA, int m, int *tauB, int n,
+                                    int *plan_host) {
   __shared__ int s_eff;
   if (threadIdx.x == 0) {
     int sv = s_base;
@@ -354,6 +355,7 @@ __global__ void ozaki_decide_kernel(const double *statA, const double *statB, in
       sv = s_hi;
     s_eff = sv;
     *s_dev = sv;
+    if (plan_host) *plan_host = sv;  // mapped pinned word, read after the call's event
   }
   __syncthreads();
   if (s_eff == s_base) return;
@@ -982,6 +984,12 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                       g_aside.tA == tA && g_aside.s == s_base && g_aside.H == t.H &&
                       g_aside.Y == (const void *)Yall && g_aside.sc == (const void *)sc;
   const bool reuse_a = same_a && g_aside.covers(r0, r0 + m);
+  // The count actually used is known on the device only: the decide kernel
+  // stores it straight into mapped pinned memory (a copy would queue behind
+  // the host pipeline's large copy-outs on the same copy engine), read by
+  // b2_ozaki_last_plan after plan_ev.
+  int *plan_word = (int *)((uint8_t *)cx->pinned + 64);
+  int *plan_dev = cx->pinned_dev ? (int *)((uint8_t *)cx->pinned_dev + 64) : nullptr;
   if (adaptive) B2_CUDA_TRY(cudaMemsetAsync(stat, 0, 4 * sizeof(double), st));
   if (!reuse_a)
     rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
@@ -992,7 +1000,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
     B2_PROF("ozaki_decide", st);
     ozaki_decide_kernel<<<1, 1024, 0, st>>>(stat, stat + 2, adaptive && s_max > s_base ? 1 : 0,
                                             s_base, s_max, dH, OZ_LOG2_RHO_MIN, s_dev, sigA, m,
-                                            tauB, n);
+                                            tauB, n, plan_dev);
     B2_CUDA_TRY(cudaGetLastError());
   }
 
@@ -1031,10 +1039,8 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                        ldc, A, asr, ask, B, bsk, bsr, k, st);
     B2_CUDA_TRY(cudaGetLastError());
   }
-  // The count actually used is known on the device only: copy it to pinned
-  // memory behind an event, read by b2_ozaki_last_plan.
-  int *plan_word = (int *)((uint8_t *)cx->pinned + 64);
-  B2_CUDA_TRY(cudaMemcpyAsync(plan_word, s_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (!plan_dev)
+    B2_CUDA_TRY(cudaMemcpyAsync(plan_word, s_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
   B2_CUDA_TRY(cudaEventRecord(cx->plan_ev, st));
   if (rows_view && !reuse_a) {
     if (!same_a) {
@@ -1191,7 +1197,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   if (rc != B2_OK) return rc;
   // fixed count (no statistics): the kernel only stores s
   ozaki_decide_kernel<<<1, 32, 0, st>>>(nullptr, nullptr, 0, s, s, 0, 0.0, s_dev, sigA, m, tauB,
-                                        n);
+                                        n, nullptr);
   B2_CUDA_TRY(cudaGetLastError());
   {
     dim3 grid((k + 63) / 64, (m + 31) / 32);
