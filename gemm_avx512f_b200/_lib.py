@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
     L.dtrsm_.argtypes = [pc, pc, pc, pc, pi, pi, p, p, pi, p, pi]
     L.dtrsm_.restype = None
     L.b2_dgemm.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, i, p]
+    L.b2_dgemm_multi.argtypes = [i, p, ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, i]
     L.b2_sgemm.argtypes = [ch, ch, i, i, i, f, p, i, p, i, f, p, i, i, p]
     L.b2_dgemm_dd.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, p, p, i, p]
     L.b2_dtrsm.argtypes = [ch, ch, ch, ch, i, i, d, p, i, p, i, i, i, p]
@@ -125,7 +126,7 @@ def lib() -> C.CDLL:
     L.b2_launch_count.restype = C.c_longlong
     L.b2_profile_enable.argtypes = [i]
     L.b2_profile_report.argtypes = [C.c_char_p, i]
-    for nm in ("b2_dgemm", "b2_sgemm", "b2_dgemm_dd", "b2_dtrsm", "b2_zgemm3m", "b2_cgemm3m",
+    for nm in ("b2_dgemm", "b2_dgemm_multi", "b2_sgemm", "b2_dgemm_dd", "b2_dtrsm", "b2_zgemm3m", "b2_cgemm3m",
                "b2_dgemm_error", "b2_device_error", "b2_set_dgemm_method", "b2_set_sgemm_method"):
         getattr(L, nm).restype = i
     _lib = L

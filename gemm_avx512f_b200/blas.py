@@ -73,6 +73,17 @@ def dgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
     return c
 
 
+def dgemm_multi(devices, transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc,
+                method="default", slices=0):
+    """``dgemm_`` on host arrays split by columns of C over the GPUs in
+    ``devices`` (an index may repeat); see b2_dgemm_multi."""
+    dv = (C.c_int * len(devices))(*[int(d) for d in devices])
+    check(lib().b2_dgemm_multi(len(devices), C.addressof(dv), _c(transa), _c(transb), m, n, k,
+                               alpha, _addr(a), lda, _addr(b), ldb, beta, _addr(c), ldc,
+                               METHODS[method], int(slices)), "b2_dgemm_multi")
+    return c
+
+
 def sgemm(transa, transb, m, n, k, alpha, a, lda, b, ldb, beta, c, ldc):
     """``sgemm_`` (src/gemm_driver.c:116 without -DDOUBLE)."""
     al, be = C.c_float(alpha), C.c_float(beta)

@@ -15,6 +15,8 @@
 #endif
 
 #include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -630,6 +632,144 @@ static int check_trsm(char side, char uplo, char transa, char diag, int m, int n
   return *info ? B2_ERR_ARG : B2_OK;
 }
 
+// ------------------------------------------------ sharded multi-GPU DGEMM --
+// A host-operand DGEMM split over several GPUs of one node: C's columns are
+// cut into one contiguous block per listed device and each block runs through
+// the drop-in path (copy pipeline, method dispatch) on its own device.  There
+// is no exchange between the shards: every device receives A and its columns
+// of B and C, so no collective or peer memory access is involved.
+//
+// Each (device, occurrence) slot has one persistent host thread, so the
+// library context of the shard (streams, events, grow-only workspaces) is
+// created on its device at the first call and reused by later calls.  The
+// threads are detached and idle on a condition variable between calls.
+namespace {
+struct ShardWorker {
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::function<int()> task;
+  bool busy = false, done = false;
+  int result = B2_OK;
+};
+std::mutex g_shard_mu;                  // one sharded call at a time
+std::vector<ShardWorker *> g_shard_workers;  // live until the process exits
+
+void shard_worker_loop(ShardWorker *w) {
+  cudaSetDevice(w->device);
+  for (;;) {
+    std::function<int()> t;
+    {
+      std::unique_lock<std::mutex> lk(w->mu);
+      w->cv.wait(lk, [&] { return w->busy && !w->done; });
+      t = w->task;
+    }
+    const int r = t();
+    {
+      std::lock_guard<std::mutex> lk(w->mu);
+      w->result = r;
+      w->done = true;
+    }
+    w->cv.notify_all();
+  }
+}
+
+// The occurrence-th worker bound to `device` (created on first use).
+ShardWorker *shard_worker(int device, int occurrence) {
+  int seen = 0;
+  for (ShardWorker *w : g_shard_workers)
+    if (w->device == device && seen++ == occurrence) return w;
+  ShardWorker *w = new ShardWorker();
+  w->device = device;
+  std::thread(shard_worker_loop, w).detach();
+  g_shard_workers.push_back(w);
+  return w;
+}
+
+// Devices listed in B2_DEVICES ("0,1,2,3"), read once; fewer than two means
+// dgemm_ does not shard.
+const std::vector<int> &env_devices() {
+  static const std::vector<int> devs = [] {
+    std::vector<int> v;
+    if (const char *e = getenv("B2_DEVICES")) {
+      const char *q = e;
+      while (*q) {
+        char *end = nullptr;
+        const long d = strtol(q, &end, 10);
+        if (end == q) break;
+        if (d >= 0 && d < 1024) v.push_back((int)d);
+        q = *end == ',' ? end + 1 : end;
+        if (*end != ',') break;
+      }
+    }
+    return v;
+  }();
+  return devs;
+}
+}  // namespace
+
+// B2_OK when every listed device exists and is an sm_100-class GPU.
+int check_shard_devices(int ndev, const int *devices) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return B2_ERR_NO_DEVICE;
+  }
+  for (int j = 0; j < ndev; ++j) {
+    cudaDeviceProp p;
+    if (devices[j] < 0 || devices[j] >= count ||
+        cudaGetDeviceProperties(&p, devices[j]) != cudaSuccess || p.major < 10) {
+      (void)cudaGetLastError();
+      return B2_ERR_ARG;
+    }
+  }
+  return B2_OK;
+}
+
+// Runs the sharded product; arguments are already checked (host operands,
+// valid devices).  Returns the first failing shard's status, in shard order.
+int dgemm_sharded(int ndev, const int *devices, char ta, char tb, int m, int n, int k,
+                  double alpha, const double *a, int lda, const double *b, int ldb, double beta,
+                  double *c, int ldc, int method, int slices) {
+  std::lock_guard<std::mutex> guard(g_shard_mu);
+  const int shards = ndev < n ? ndev : n;
+  const int base = n / shards, rem = n % shards;
+  std::vector<ShardWorker *> ws(shards);
+  int j0 = 0;
+  for (int j = 0; j < shards; ++j) {
+    int occ = 0;
+    for (int i = 0; i < j; ++i) occ += devices[i] == devices[j];
+    ShardWorker *w = shard_worker(devices[j], occ);
+    const int nj = base + (j < rem ? 1 : 0);
+    const double *bj = notrans(tb) ? b + (size_t)j0 * ldb : b + j0;
+    double *cj = c + (size_t)j0 * ldc;
+    {
+      std::lock_guard<std::mutex> lk(w->mu);
+      w->task = [=]() {
+        return gemm_dropin<double>(ta, tb, m, nj, k, alpha, a, lda, bj, ldb, beta, cj, ldc,
+                                   [&](const double *A, int la, const double *B, int lb,
+                                       double *C, int lc, int mrows, int ncols, cudaStream_t s) {
+                                     return dgemm_device(ta, tb, mrows, ncols, k, alpha, A, la,
+                                                         B, lb, beta, C, lc, method, slices, s);
+                                   });
+      };
+      w->busy = true;
+      w->done = false;
+    }
+    w->cv.notify_all();
+    ws[j] = w;
+    j0 += nj;
+  }
+  int st = B2_OK;
+  for (ShardWorker *w : ws) {
+    std::unique_lock<std::mutex> lk(w->mu);
+    w->cv.wait(lk, [&] { return w->done; });
+    w->busy = false;
+    if (st == B2_OK && w->result != B2_OK) st = w->result;
+  }
+  return st;
+}
+
 }  // namespace b2
 
 using namespace b2;
@@ -694,6 +834,27 @@ void dgemm_(const char *transa, const char *transb, const int *m, const int *n, 
   }
   const char ta = *transa, tb = *transb;
   const double al = *alpha, be = *beta;
+  // B2_DEVICES lists two or more GPUs: a large product on host operands is
+  // sharded over them by columns of C (checked arguments only).
+  const std::vector<int> &devs = env_devices();
+  if (devs.size() >= 2 && 2.0 * *m * (double)*n * *k >= 4294967296.0 && *n >= (int)devs.size() &&
+      arg_mode() == B2_ARGS_BLAS) {
+    int info = 0;
+    if (check_gemm(ta, tb, *m, *n, *k, *lda, *ldb, *ldc, a, b, c, &info) == B2_OK &&
+        !is_device_ptr(a) && !is_device_ptr(b) && !is_device_ptr(c)) {
+      Ctx *cx = ctx();
+      if (!cx) { set_status(B2_ERR_NO_DEVICE); return; }
+      const int dst = check_shard_devices((int)devs.size(), devs.data());
+      if (dst != B2_OK) {  // a device named in B2_DEVICES is missing: fail loudly
+        if (getenv("B2_VERBOSE")) fprintf(stderr, "b2blas: B2_DEVICES names an unusable device\n");
+        set_status(dst, 0);
+        return;
+      }
+      set_status(dgemm_sharded((int)devs.size(), devs.data(), ta, tb, *m, *n, *k, al, a, *lda, b,
+                               *ldb, be, c, *ldc, cx->dgemm_method, cx->dgemm_slices));
+      return;
+    }
+  }
   gemm_dropin<double>(ta, tb, *m, *n, *k, al, a, *lda, b, *ldb, be, c, *ldc,
                       [&](const double *A, int la, const double *B, int lb, double *C, int lc,
                           int mrows, int ncols, cudaStream_t s) {
@@ -857,6 +1018,39 @@ int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha, const 
   }
   st = dgemm_device(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method, slices,
                     pick_stream(c, stream));
+  set_status(st);
+  return st;
+}
+
+int b2_dgemm_multi(int ndev, const int *devices, char transa, char transb, int m, int n, int k,
+                   double alpha, const double *A, int lda, const double *B, int ldb, double beta,
+                   double *C, int ldc, int method, int slices) {
+  int info = 0;
+  int st = check_gemm(transa, transb, m, n, k, lda, ldb, ldc, A, B, C, &info);
+  if (st != B2_OK) { set_status(st, info); return st; }
+  if (ndev < 1 || ndev > 64 || !devices ||
+      !(method == B2_METHOD_DEFAULT || method == B2_METHOD_FP64 || method == B2_METHOD_OZAKI ||
+        method == B2_METHOD_AUTO) ||
+      slices < 0 || slices > B2_MAX_MODULI) {
+    set_status(B2_ERR_ARG, 0);
+    return B2_ERR_ARG;
+  }
+  st = check_shard_devices(ndev, devices);
+  if (st != B2_OK) { set_status(st, 0); return st; }
+  // host memory only: a shard's kernels never read another GPU's memory
+  if (is_device_ptr(C) || is_device_ptr(A) || is_device_ptr(B)) {
+    set_status(B2_ERR_ARG, is_device_ptr(C) ? 12 : (is_device_ptr(A) ? 7 : 9));
+    return B2_ERR_ARG;
+  }
+  if (m == 0 || n == 0) { set_status(B2_OK); return B2_OK; }
+  if (method == B2_METHOD_DEFAULT) {
+    Ctx *c = ctx();
+    if (!c) { set_status(B2_ERR_NO_DEVICE); return B2_ERR_NO_DEVICE; }
+    method = c->dgemm_method;
+    if (slices == 0) slices = c->dgemm_slices;
+  }
+  st = dgemm_sharded(ndev, devices, transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                     method, slices);
   set_status(st);
   return st;
 }

@@ -143,6 +143,25 @@ B2_API int b2_dgemm(char transa, char transb, int m, int n, int k, double alpha,
              int lda, const double *B, int ldb, double beta, double *C, int ldc, int method,
              int slices, void *stream);
 
+/* dgemm_ (src/gemm_driver.c:116, where the reference splits N over OpenMP
+ * threads at :136-149) split over several GPUs of one node: C's columns are
+ * cut into ndev contiguous blocks (sizes differ by at most one column) and
+ * block j is computed on GPU devices[j] through the drop-in host path (copy
+ * pipeline, method and modulus count as given; B2_METHOD_DEFAULT = the calling
+ * thread's method).  No data crosses between GPUs: each receives A and its
+ * columns of B and C.  Host memory only (device or managed pointers return
+ * B2_ERR_ARG, info 7/9/12); a device index may repeat (several shards on one
+ * GPU).  Synchronous; one persistent host thread per (device, occurrence)
+ * keeps its streams and workspaces between calls; sharded calls from several
+ * host threads are serialised.  Argument errors use dgemm_'s positions;
+ * ndev outside 1..64, an unknown or pre-sm_100 device, a bad method or slice
+ * count give B2_ERR_ARG with info 0.  dgemm_ itself shards a product of at
+ * least 2^32 flops on host operands this way when the environment variable
+ * B2_DEVICES lists two or more devices ("0,1,2,3"). */
+B2_API int b2_dgemm_multi(int ndev, const int *devices, char transa, char transb, int m, int n,
+                          int k, double alpha, const double *A, int lda, const double *B,
+                          int ldb, double beta, double *C, int ldc, int method, int slices);
+
 /* Plan of the last Ozaki DGEMM on this thread: out[0] = modulus (slice)
  * count, out[1] = number of K chunks (K is cut at 65536 per exact INT32 pass).
  * With slices = 0 the count (15, or 16 for heavy-tailed rows) is chosen on the

@@ -127,3 +127,20 @@ def test_openblas_argument_mode(capfd):
         assert "LDA < M" in capfd.readouterr().out
     finally:
         assert L.b2_set_arg_mode(prev) == 1
+
+
+@pytest.mark.parametrize("ndev,devs,args,info", [
+    (0, [0], {}, 0), (65, [0] * 65, {}, 0), (2, [0, 0], dict(m=-1), 3), (2, [0, 0], dict(ldc=4), 13)])
+def test_dgemm_multi_argument_errors(ndev, devs, args, info):
+    # checked before any device is looked at
+    m, n, k = args.get("m", 5), args.get("n", 6), 7
+    ldc = args.get("ldc", 5)
+    a, b = np.ones((5, 7), order="F"), np.ones((7, 6), order="F")
+    c = np.full((5, 6), 3.0, order="F")
+    dv = (C.c_int * len(devs))(*devs)
+    st = _lib.lib().b2_dgemm_multi(ndev, C.addressof(dv), b"N", b"N", m, n, k, 1.0,
+                                   a.ctypes.data, 5, b.ctypes.data, 7, 0.0, c.ctypes.data, ldc,
+                                   0, 0)
+    assert st == _lib.B2_ERR_ARG
+    assert _lib.lib().b2_last_info() == info
+    assert (c == 3.0).all()
