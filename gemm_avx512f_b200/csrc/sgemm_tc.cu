@@ -65,12 +65,25 @@ __global__ void __launch_bounds__(256)
       small[j] = __float2bfloat16_rn(v - __bfloat162float(h));
     }
   }
+  // 16-byte stores: each thread's 8 elements are contiguous and 16-B aligned
+  // (kp is a multiple of 128 bytes, k0 of 64 elements, kg of 8), so a term is
+  // two float4 (FP32) or one 8 x BF16 pack; scalar stores left every warp
+  // store instruction touching 32 sectors.
   T *row = out + (long long)r * terms * kp;
   for (int t = 0; t < terms; ++t) {
     const T *src = ((pattern >> t) & 1u) ? small : big;
     T *dst = row + (long long)t * kp + k0 + kg;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) dst[j] = src[j];
+    if constexpr (sizeof(T) == 4) {
+      reinterpret_cast<float4 *>(dst)[0] = make_float4(src[0], src[1], src[2], src[3]);
+      reinterpret_cast<float4 *>(dst)[1] = make_float4(src[4], src[5], src[6], src[7]);
+    } else {
+      uint4 p;
+      p.x = (uint32_t)__bfloat16_as_ushort(src[0]) | ((uint32_t)__bfloat16_as_ushort(src[1]) << 16);
+      p.y = (uint32_t)__bfloat16_as_ushort(src[2]) | ((uint32_t)__bfloat16_as_ushort(src[3]) << 16);
+      p.z = (uint32_t)__bfloat16_as_ushort(src[4]) | ((uint32_t)__bfloat16_as_ushort(src[5]) << 16);
+      p.w = (uint32_t)__bfloat16_as_ushort(src[6]) | ((uint32_t)__bfloat16_as_ushort(src[7]) << 16);
+      *reinterpret_cast<uint4 *>(dst) = p;
+    }
   }
 }
 
