@@ -1,6 +1,7 @@
 """Measurement suite for every workload of the hot path, on one B200.
 
     python -m gemm_avx512f_b200.suite [--only dgemm,sgemm,ozaki,grouped,complex,trsm,select]
+                                      [--sgemm-shape MxNxK ...]
                                       [--quick] [--out results.jsonl]
 
 One JSON line per measurement.  Each line names the workload (shapes, seed,
@@ -127,6 +128,8 @@ def run_sgemm(ctx, out, quick):
     shapes = [(2048, 2048, 2048), (4096, 4096, 4096), (8192, 8192, 8192), (8192, 256, 8192)]
     if quick:
         shapes = [(4096, 4096, 4096), (8192, 256, 8192)]
+    if ctx.get("sgemm_shapes"):
+        shapes = ctx["sgemm_shapes"]
     g = torch.Generator(device=dev)
     g.manual_seed(1)
     bound = {"fp32": ("fp32 SIMT (nominal)", P["fp32_tflops"], 1),
@@ -345,6 +348,8 @@ def main(argv=None) -> int:
     ap.add_argument("--only", default=",".join(RUNNERS))
     ap.add_argument("--quick", action="store_true", help="smaller sizes (a smoke run)")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--sgemm-shape", action="append", default=[],
+                    help="MxNxK for the sgemm runner (repeatable; default: the config-2 shapes)")
     args = ap.parse_args(argv)
     import torch
 
@@ -352,7 +357,8 @@ def main(argv=None) -> int:
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     ctx = {"torch": torch, "dev": dev, "stream": stream, "timer": Timer(torch, stream),
-           "peaks": peaks()}
+           "peaks": peaks(),
+           "sgemm_shapes": [tuple(int(v) for v in sh.lower().split("x")) for sh in args.sgemm_shape]}
     out = open(args.out, "w") if args.out else None
     emit(out, {"peaks": ctx["peaks"], "gpu": torch.cuda.get_device_name(0)})
     for name in args.only.split(","):
