@@ -8,10 +8,13 @@
 //                       C = Ab Bb + Ab Bs + As Bb                (kind::tf32)
 //   BF16X3  3 products: A = Ah + Al, B = Bh + Bl (each BF16),
 //                       C = Ah Bh + Ah Bl + Al Bh                (kind::f16, bf16 in)
-// The split terms are laid side by side along K ([Bb|Bs|Bb] against
-// [Ab|Ab|As]), so every method is ONE GEMM over K' = terms * Kp on the
-// engine in umma.cuh; the split/convert kernel is the only extra pass.  Each
-// K segment is padded with zeros to a 128-byte K block.
+// Every method is ONE GEMM over K' = terms * Kp on the engine in umma.cuh;
+// the split/convert kernel is the only extra pass.  For three terms each
+// operand stores two segments, [big | small], each padded with zeros to a
+// 128-byte K block, and the engine's three-term interleave reads K' block j
+// as term j % 3 of K block j / 3: (Bb, Ab), (Bs, Ab), (Bb, As).  The big part
+// used by two terms is written once and read from DRAM once (its second load
+// is an L2 hit a few K' blocks later).
 #include <cuda_bf16.h>
 
 #include "b2_methods.cuh"
@@ -204,28 +207,33 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
   const int terms = (method == B2_METHOD_TF32) ? 1 : 3;
   const int esz = bf16 ? 2 : 4;
   const int kp = (int)round_up(k, 128 / esz);
-  const long long kt = (long long)terms * kp;
-  void *Yp = workspace(cx, WS_SPLIT_Y, (size_t)m * kt * esz);
-  void *Xp = workspace(cx, WS_SPLIT_X, (size_t)n * kt * esz);
+  const long long kt = (long long)terms * kp;               // K' of the one GEMM
+  const int segs = terms == 3 ? 2 : 1;                      // stored segments per row
+  const long long ks_ = (long long)segs * kp;
+  void *Yp = workspace(cx, WS_SPLIT_Y, (size_t)m * ks_ * esz);
+  void *Xp = workspace(cx, WS_SPLIT_X, (size_t)n * ks_ * esz);
   if (!Yp || !Xp) return B2_ERR_NOMEM;
-  // A side gets [big, big, small], B side [big, small, big]
-  const unsigned patA = 0x4u, patB = 0x2u;
+  // stored segments: [big] or [big, small]; terms read (Bb, Ab), (Bs, Ab), (Bb, As)
+  const unsigned pat = 0x2u;                      // segment 1 holds the small part
+  const unsigned segX = 0x2u, segY = 0x4u;        // term -> segment, B side / A side
   int rc;
   if (bf16) {
-    rc = run_split<__nv_bfloat16>(A, asr, ask, m, k, kp, terms, patA, (__nv_bfloat16 *)Yp, s);
+    rc = run_split<__nv_bfloat16>(A, asr, ask, m, k, kp, segs, pat, (__nv_bfloat16 *)Yp, s);
     if (rc == B2_OK)
-      rc = run_split<__nv_bfloat16>(B, bsr, bsk, n, k, kp, terms, patB, (__nv_bfloat16 *)Xp, s);
+      rc = run_split<__nv_bfloat16>(B, bsr, bsk, n, k, kp, segs, pat, (__nv_bfloat16 *)Xp, s);
   } else {
-    rc = run_split<float>(A, asr, ask, m, k, kp, terms, patA, (float *)Yp, s);
-    if (rc == B2_OK) rc = run_split<float>(B, bsr, bsk, n, k, kp, terms, patB, (float *)Xp, s);
+    rc = run_split<float>(A, asr, ask, m, k, kp, segs, pat, (float *)Yp, s);
+    if (rc == B2_OK) rc = run_split<float>(B, bsr, bsk, n, k, kp, segs, pat, (float *)Xp, s);
   }
   if (rc != B2_OK) return rc;
   const int kind = bf16 ? umma::KIND_BF16 : umma::KIND_TF32;
   CUtensorMap tmX, tmY;
-  rc = umma::make_kmajor_map(&tmX, kind, Xp, kt, n, 1, kt * esz, (long long)n * kt * esz, umma::BM);
+  rc = umma::make_kmajor_map(&tmX, kind, Xp, ks_, n, 1, ks_ * esz, (long long)n * ks_ * esz,
+                             umma::BM);
   if (rc == B2_OK)
-    rc = umma::make_kmajor_map(&tmY, kind, Yp, kt, m, 1, kt * esz, (long long)m * kt * esz, 256);
+    rc = umma::make_kmajor_map(&tmY, kind, Yp, ks_, m, 1, ks_ * esz, (long long)m * ks_ * esz, 256);
   if (rc != B2_OK) return rc;
+  const int seg_kb = terms == 3 ? (int)((long long)kp * esz / umma::KBLOCK_BYTES) : 0;
   const long long tiles = ((n + umma::BM - 1) / umma::BM) * (long long)((m + 255) / 256);
   const int kblocks = (int)((kt * esz + umma::KBLOCK_BYTES - 1) / umma::KBLOCK_BYTES);
   int S = choose_ksplit(tiles, kblocks, cx->sm_count);
@@ -238,9 +246,11 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
     F32Epi epi{C, ldc, m, n, alpha, beta};
     if (bf16)
       return umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
-                                                    cx->derr, s, "sgemm_umma_bf16");
+                                                    cx->derr, s, "sgemm_umma_bf16", 0, nullptr,
+                                                    1, seg_kb, segX, segY);
     return umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
-                                                  cx->derr, s, "sgemm_umma_tf32");
+                                                  cx->derr, s, "sgemm_umma_tf32", 0, nullptr, 1,
+                                                  seg_kb, segX, segY);
   }
   // Split-K: S partial products of K ranges, then one fixed-order reduction.
   const int ldw = (int)round_up(m, 256);  // whole 256-column tiles stay in bounds
@@ -249,9 +259,11 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
   if (!W) return B2_ERR_NOMEM;
   F32PartialEpi pe{W, plane, ldw, m, n};
   rc = bf16 ? umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, pe, cx->sm_count,
-                                                     cx->derr, s, "sgemm_umma_bf16", 0, nullptr, S)
+                                                     cx->derr, s, "sgemm_umma_bf16", 0, nullptr, S,
+                                                     seg_kb, segX, segY)
             : umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, pe, cx->sm_count,
-                                                     cx->derr, s, "sgemm_umma_tf32", 0, nullptr, S);
+                                                     cx->derr, s, "sgemm_umma_tf32", 0, nullptr, S,
+                                                     seg_kb, segX, segY);
   if (rc != B2_OK) return rc;
   dim3 grid((unsigned)((m + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
   B2_PROF("sgemm_splitk_reduce", s);

@@ -204,6 +204,13 @@ struct Problem {
   int tiles_p, tiles_q;
   int group;       // tile rasterisation: GROUP rows of P tiles share a sweep over Q
   int *derr;       // device error word
+  // Three-term interleave (0 = off): K' block j is term j % 3 of K block j / 3;
+  // the operands store 2 segments of seg_kb K blocks (0 = big, 1 = small) and
+  // bit t of seg_x / seg_y names the segment term t reads.  The big part that
+  // two terms share is read from DRAM once: its second load follows the first
+  // within three K' blocks and is served by L2.
+  int seg_kb;
+  unsigned seg_x, seg_y;
 };
 
 template <int BN, int STAGES>
@@ -302,8 +309,14 @@ __global__ void __launch_bounds__(THREADS, 1)
           const uint32_t sx = base + stage * L::STAGE_BYTES;
           const uint32_t sy = sx + L::X_BYTES;
           mbar_expect_tx(full_bar(stage), L::STAGE_BYTES);
-          tma_load_3d(sx, &tmX, full_bar(stage), kb * kcoord, tp * BM, b);
-          tma_load_3d(sy, &tmY, full_bar(stage), kb * kcoord, tq * BN, b);
+          int kx = kb * kcoord, ky = kx;
+          if (pr.seg_kb) {
+            const int kq = kb / 3, tt = kb - 3 * kq;
+            kx = ((int)((pr.seg_x >> tt) & 1u) * pr.seg_kb + kq) * kcoord;
+            ky = ((int)((pr.seg_y >> tt) & 1u) * pr.seg_kb + kq) * kcoord;
+          }
+          tma_load_3d(sx, &tmX, full_bar(stage), kx, tp * BM, b);
+          tma_load_3d(sy, &tmY, full_bar(stage), ky, tq * BN, b);
           ++issued;
           if (++stage == STAGES) { stage = 0; phase ^= 1u; }
         }
@@ -699,11 +712,14 @@ template <int KIND, int BN, int STAGES, class Epi>
 int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
            int nbatch, const Epi &epi, int sm_count, int *derr, cudaStream_t s,
            const char *prof_name, int max_ctas = 0, const int *nbatch_dev = nullptr,
-           int ksplit = 1) {
+           int ksplit = 1, int seg_kb = 0, unsigned seg_x = 0, unsigned seg_y = 0) {
   using L = SmemLayout<BN, STAGES>;
   Problem pr;
   pr.P = P;
   pr.Q = Q;
+  pr.seg_kb = seg_kb;
+  pr.seg_x = seg_x;
+  pr.seg_y = seg_y;
   pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
   pr.nbatch = nbatch;
   pr.nbatch_dev = nbatch_dev;
@@ -748,6 +764,8 @@ int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, lo
   pr.nbatch_dev = nbatch_dev;
   pr.ksplit = 1;
   pr.kb_per_split = pr.kblocks;
+  pr.seg_kb = 0;  // the pair engine reads K' linearly
+  pr.seg_x = pr.seg_y = 0;
   pr.tiles_p = (P + PAIR_BM - 1) / PAIR_BM;
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;
