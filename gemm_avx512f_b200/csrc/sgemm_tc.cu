@@ -33,59 +33,110 @@ __device__ __forceinline__ float tf32_round(float x) {  // round to nearest, tie
 // Writes `terms` K-segments per row of the operand viewed as R x K (element
 // (r,k) at X[r*sr + k*sk]) into out[r][terms*kp] (elements of type T).
 // pattern: which split part each segment holds (0 = big/high, 1 = small/low).
+// vec (checked on the host: X 16-byte aligned and the strided dimension a
+// multiple of 4 elements, unit stride along the other): 16-byte loads of 4
+// consecutive rows (ROWCONT) or 4 consecutive k; otherwise scalar loads.
 template <typename T, bool ROWCONT>
 __global__ void __launch_bounds__(256)
     split_kernel(const float *__restrict__ X, long long sr, long long sk, int R, int K, int kp,
-                 int terms, unsigned pattern, T *__restrict__ out) {
+                 int terms, unsigned pattern, T *__restrict__ out, int vec) {
   __shared__ float tile[32][65];
   const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32;
   const int tid = threadIdx.x;
+  if (vec) {
 #pragma unroll
-  for (int e = 0; e < 8; ++e) {
-    const int idx = tid + 256 * e;
-    int rr, kk;
-    if (ROWCONT) { rr = idx & 31; kk = idx >> 5; } else { kk = idx & 63; rr = idx >> 6; }
-    const int r = r0 + rr, k = k0 + kk;
-    float v = 0.f;
-    if (r < R && k < K) v = __ldg(X + (long long)r * sr + (long long)k * sk);
-    tile[rr][kk] = v;
-  }
-  __syncthreads();
-  const int rr = tid >> 3, kg = (tid & 7) * 8;
-  const int r = r0 + rr;
-  if (r >= R || k0 + kg >= kp) return;  // pad columns [K, kp) are written as zeros below
-  T big[8], small[8];
+    for (int e = 0; e < 2; ++e) {
+      const int idx = tid + 256 * e;
+      float v[4] = {0.f, 0.f, 0.f, 0.f};
+      if (ROWCONT) {  // 32 rows x 64 k: 8 float4 per k column
+        const int kk = idx >> 3, rr = (idx & 7) * 4;
+        const int r = r0 + rr, k = k0 + kk;
+        if (k < K) {
+          const float *src = X + r + (long long)k * sk;
+          if (r + 3 < R) {
+            const float4 q = __ldg(reinterpret_cast<const float4 *>(src));
+            v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+          } else {
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const float v = (k0 + kg + j < K) ? tile[rr][kg + j] : 0.f;
-    if constexpr (sizeof(T) == 4) {
-      const float b = tf32_round(v);
-      big[j] = b;
-      small[j] = tf32_round(v - b);
-    } else {
-      const __nv_bfloat16 h = __float2bfloat16_rn(v);
-      big[j] = h;
-      small[j] = __float2bfloat16_rn(v - __bfloat162float(h));
+            for (int j = 0; j < 4; ++j)
+              if (r + j < R) v[j] = __ldg(src + j);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tile[rr + j][kk] = v[j];
+      } else {  // 32 rows x 64 k: 16 float4 per row
+        const int rr = idx >> 4, kk = (idx & 15) * 4;
+        const int r = r0 + rr, k = k0 + kk;
+        if (r < R) {
+          const float *src = X + (long long)r * sr + k;
+          if (k + 3 < K) {
+            const float4 q = __ldg(reinterpret_cast<const float4 *>(src));
+            v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+              if (k + j < K) v[j] = __ldg(src + j);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) tile[rr][kk + j] = v[j];
+      }
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      const int idx = tid + 256 * e;
+      int rr, kk;
+      if (ROWCONT) { rr = idx & 31; kk = idx >> 5; } else { kk = idx & 63; rr = idx >> 6; }
+      const int r = r0 + rr, k = k0 + kk;
+      float v = 0.f;
+      if (r < R && k < K) v = __ldg(X + (long long)r * sr + (long long)k * sk);
+      tile[rr][kk] = v;
     }
   }
-  // 16-byte stores: each thread's 8 elements are contiguous and 16-B aligned
-  // (kp is a multiple of 128 bytes, k0 of 64 elements, kg of 8), so a term is
-  // two float4 (FP32) or one 8 x BF16 pack; scalar stores left every warp
-  // store instruction touching 32 sectors.
+  __syncthreads();
+  const int rr = tid >> 3, q = tid & 7;
+  const int r = r0 + rr;
+  if (r >= R) return;
   T *row = out + (long long)r * terms * kp;
-  for (int t = 0; t < terms; ++t) {
-    const T *src = ((pattern >> t) & 1u) ? small : big;
-    T *dst = row + (long long)t * kp + k0 + kg;
-    if constexpr (sizeof(T) == 4) {
-      reinterpret_cast<float4 *>(dst)[0] = make_float4(src[0], src[1], src[2], src[3]);
-      reinterpret_cast<float4 *>(dst)[1] = make_float4(src[4], src[5], src[6], src[7]);
-    } else {
-      uint4 p;
-      p.x = (uint32_t)__bfloat16_as_ushort(src[0]) | ((uint32_t)__bfloat16_as_ushort(src[1]) << 16);
-      p.y = (uint32_t)__bfloat16_as_ushort(src[2]) | ((uint32_t)__bfloat16_as_ushort(src[3]) << 16);
-      p.z = (uint32_t)__bfloat16_as_ushort(src[4]) | ((uint32_t)__bfloat16_as_ushort(src[5]) << 16);
-      p.w = (uint32_t)__bfloat16_as_ushort(src[6]) | ((uint32_t)__bfloat16_as_ushort(src[7]) << 16);
-      *reinterpret_cast<uint4 *>(dst) = p;
+  // 16-byte stores of 16-byte groups of consecutive k: FP32 writes groups
+  // k0 + 4q and k0 + 32 + 4q (the second only where kp reaches it; kp is a
+  // multiple of 32), so each store instruction covers whole 128-byte lines
+  // of a row; BF16 writes one group of 8 at k0 + 8q (kp is a multiple of 64).
+  // Pad columns [K, kp) are written as zeros.
+  constexpr int GW = sizeof(T) == 4 ? 4 : 8;   // elements per 16-byte group
+  constexpr int NG = sizeof(T) == 4 ? 2 : 1;   // groups per thread
+#pragma unroll
+  for (int g = 0; g < NG; ++g) {
+    const int kl = (sizeof(T) == 4) ? g * 32 + 4 * q : 8 * q;  // offset within the 64-k tile
+    if (k0 + kl >= kp) break;
+    T big[GW], small[GW];
+#pragma unroll
+    for (int j = 0; j < GW; ++j) {
+      const float v = (k0 + kl + j < K) ? tile[rr][kl + j] : 0.f;
+      if constexpr (sizeof(T) == 4) {
+        const float bv = tf32_round(v);
+        big[j] = bv;
+        small[j] = tf32_round(v - bv);
+      } else {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        big[j] = h;
+        small[j] = __float2bfloat16_rn(v - __bfloat162float(h));
+      }
+    }
+    for (int t = 0; t < terms; ++t) {
+      const T *src = ((pattern >> t) & 1u) ? small : big;
+      T *dst = row + (long long)t * kp + k0 + kl;
+      if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(src[0], src[1], src[2], src[3]);
+      } else {
+        uint4 p;
+        p.x = (uint32_t)__bfloat16_as_ushort(src[0]) | ((uint32_t)__bfloat16_as_ushort(src[1]) << 16);
+        p.y = (uint32_t)__bfloat16_as_ushort(src[2]) | ((uint32_t)__bfloat16_as_ushort(src[3]) << 16);
+        p.z = (uint32_t)__bfloat16_as_ushort(src[4]) | ((uint32_t)__bfloat16_as_ushort(src[5]) << 16);
+        p.w = (uint32_t)__bfloat16_as_ushort(src[6]) | ((uint32_t)__bfloat16_as_ushort(src[7]) << 16);
+        *reinterpret_cast<uint4 *>(dst) = p;
+      }
     }
   }
 }
@@ -182,10 +233,14 @@ int run_split(const float *Xp, long long sr, long long sk, int R, int K, int kp,
               unsigned pattern, T *out, cudaStream_t s) {
   dim3 grid((kp + 63) / 64, (R + 31) / 32);
   B2_PROF("sgemm_split", s);
-  if (sr == 1)
-    split_kernel<T, true><<<grid, 256, 0, s>>>(Xp, sr, sk, R, K, kp, terms, pattern, out);
-  else
-    split_kernel<T, false><<<grid, 256, 0, s>>>(Xp, sr, sk, R, K, kp, terms, pattern, out);
+  const bool aligned = ((uintptr_t)Xp & 15) == 0;
+  if (sr == 1) {
+    const int vec = aligned && (sk % 4 == 0);
+    split_kernel<T, true><<<grid, 256, 0, s>>>(Xp, sr, sk, R, K, kp, terms, pattern, out, vec);
+  } else {
+    const int vec = aligned && sk == 1 && (sr % 4 == 0);
+    split_kernel<T, false><<<grid, 256, 0, s>>>(Xp, sr, sk, R, K, kp, terms, pattern, out, vec);
+  }
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
