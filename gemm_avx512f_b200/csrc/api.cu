@@ -674,14 +674,20 @@ void shard_worker_loop(ShardWorker *w) {
   }
 }
 
-// The occurrence-th worker bound to `device` (created on first use).
+// The occurrence-th worker bound to `device` (created on first use; null
+// when the host cannot start another thread).
 ShardWorker *shard_worker(int device, int occurrence) {
   int seen = 0;
   for (ShardWorker *w : g_shard_workers)
     if (w->device == device && seen++ == occurrence) return w;
   ShardWorker *w = new ShardWorker();
   w->device = device;
-  std::thread(shard_worker_loop, w).detach();
+  try {
+    std::thread(shard_worker_loop, w).detach();
+  } catch (...) {
+    delete w;
+    return nullptr;
+  }
   g_shard_workers.push_back(w);
   return w;
 }
@@ -727,19 +733,25 @@ int check_shard_devices(int ndev, const int *devices) {
 }
 
 // Runs the sharded product; arguments are already checked (host operands,
-// valid devices).  Returns the first failing shard's status, in shard order.
+// valid devices).  Returns the first failing shard's status, in shard order,
+// or B2_ERR_NOMEM when a shard's worker thread cannot be started.
 int dgemm_sharded(int ndev, const int *devices, char ta, char tb, int m, int n, int k,
                   double alpha, const double *a, int lda, const double *b, int ldb, double beta,
                   double *c, int ldc, int method, int slices) {
   std::lock_guard<std::mutex> guard(g_shard_mu);
   const int shards = ndev < n ? ndev : n;
   const int base = n / shards, rem = n % shards;
-  std::vector<ShardWorker *> ws(shards);
+  std::vector<ShardWorker *> ws;
+  int st = B2_OK;
   int j0 = 0;
   for (int j = 0; j < shards; ++j) {
     int occ = 0;
     for (int i = 0; i < j; ++i) occ += devices[i] == devices[j];
     ShardWorker *w = shard_worker(devices[j], occ);
+    if (!w) {  // no thread for this shard: finish the ones started, then fail
+      st = B2_ERR_NOMEM;
+      break;
+    }
     const int nj = base + (j < rem ? 1 : 0);
     const double *bj = notrans(tb) ? b + (size_t)j0 * ldb : b + j0;
     double *cj = c + (size_t)j0 * ldc;
@@ -757,10 +769,9 @@ int dgemm_sharded(int ndev, const int *devices, char ta, char tb, int m, int n, 
       w->done = false;
     }
     w->cv.notify_all();
-    ws[j] = w;
+    ws.push_back(w);
     j0 += nj;
   }
-  int st = B2_OK;
   for (ShardWorker *w : ws) {
     std::unique_lock<std::mutex> lk(w->mu);
     w->cv.wait(lk, [&] { return w->done; });
