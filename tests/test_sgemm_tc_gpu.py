@@ -1,7 +1,7 @@
 """GPU tests of the tensor-core SGEMM forms (1xTF32, 3xTF32, 3xBF16 on tcgen05,
 FP32 accumulation in TMEM) through the C ABI.
 
-Parity bar (north star): ||C - C_ref||_F / (K u ||A||_F ||B||_F) <= 8 against
+Parity bar: ||C - C_ref||_F / (K u ||A||_F ||B||_F) <= 8 against
 the reference sgemm_ (oracle, bit-exact restatement), with u the unit
 roundoff of the arithmetic each method actually performs: 1xTF32 rounds the
 inputs to 11 significant bits (u = 2^-11), the split forms carry ~22 (TF32)
