@@ -15,7 +15,7 @@ def op_dims(trans, rows, cols):
 
 
 def normalized(c, c_ref, k, a, b, u):
-    """||C - C_ref||_F / (K u ||A||_F ||B||_F) -- the north-star parity yardstick (<= 8)."""
+    """||C - C_ref||_F / (K u ||A||_F ||B||_F) -- the parity yardstick (<= 8)."""
     den = max(k, 1) * u * float(np.linalg.norm(a.astype(np.float64))) * float(
         np.linalg.norm(b.astype(np.float64)))
     num = float(np.linalg.norm((c.astype(np.float64) - c_ref.astype(np.float64))))
