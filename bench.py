@@ -5,7 +5,7 @@ a = u*exp(phi*g) (u ~ U[-1,1), g ~ N(0,1), seed 2), errors stated against the
 double-double product.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                    [--method ozaki|fp64] [--n 8192] [--phi 1.0] [--slices 0]
+                    [--method ozaki|fp64] [--size 8192] [--phi 1.0] [--slices 0]
 
 Prints ONE JSON line (rank 0).  ``value`` is device-timed whole-job TFLOPS with
 inputs resident in HBM; ``e2e`` is the same metric through the drop-in
@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--method", default="ozaki", choices=["ozaki", "fp64"])
-    p.add_argument("--n", type=int, default=8192)
+    p.add_argument("--size", "--n", dest="n", type=int, default=8192)
     p.add_argument("--phi", type=float, default=1.0)
     p.add_argument("--slices", type=int, default=0)
     p.add_argument("--no-cpu", action="store_true")
@@ -52,14 +52,11 @@ def parse():
 
 
 def make_inputs(n: int, phi: float, seed: int = 2):
-    """Config-3 inputs: u then g for A, then u then g for B, column-major order."""
-    rng = np.random.default_rng(seed)
-    out = []
-    for _ in range(2):
-        u = rng.uniform(-1.0, 1.0, n * n)
-        g = rng.standard_normal(n * n)
-        out.append(u * np.exp(phi * g))
-    return out[0], out[1]
+    """Emulated-DGEMM inputs a = u*exp(phi*g): u then g for A, then u then g for
+    B, flat column-major (gemm_avx512f_b200.inputs.config3)."""
+    from gemm_avx512f_b200 import inputs
+
+    return inputs.config3_flat(n, phi, seed)
 
 
 def load_peaks():
@@ -237,7 +234,7 @@ def job_tflops(world: int, flops_per_step: float, steps: int, ms: float) -> floa
     return world * flops_per_step * steps / (ms / 1e3) / 1e12
 
 
-def reference_arm(args, rank: int):
+def reference_arm(args, rank: int, world: int = 1):
     if rank != 0:
         return None
     os.environ.setdefault("OMP_NUM_THREADS", str(physical_cores()))
@@ -251,7 +248,7 @@ def reference_arm(args, rank: int):
     val = statistics.median(steps)
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "TFLOPS",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": config_block(args),
         "cpu_baseline": {"value": val, "unit": "TFLOPS", "cores": res["cores"],
@@ -399,9 +396,11 @@ def gpu_arm(args, rank: int, world: int):
         out["errors_vs_dd"] = errs
         del hi
 
-    # ---- end to end through the drop-in dgemm_ with pinned host buffers
+    # ---- end to end through the drop-in dgemm_: pinned host buffers (the
+    # headline e2e), then plain malloc'ed (pageable) ones as a BLAS caller has
     if not args.no_e2e:
         out["e2e"] = e2e_leg(args, L, a_h, b_h, method, dist, dev, world)
+        out["e2e_pageable"] = e2e_pageable_leg(args, L, a_h, b_h, method, dist, dev, world)
 
     # ---- CPU baseline (reference on the host cores), rank 0 at N=1 only
     if not args.no_cpu and rank == 0 and world == 1:
@@ -487,6 +486,39 @@ def e2e_leg(args, L, a_h, b_h, method, dist=None, dev=None, world=1):
                     "with beta == 0 C is scanned on the host (all finite, so not copied in)"}
 
 
+def e2e_pageable_leg(args, L, a_h, b_h, method, dist=None, dev=None, world=1):
+    """The same drop-in dgemm_ call on pageable host memory (numpy buffers, not
+    pinned): the driver stages every copy through its own pinned bounce
+    buffers, so the copies run slower and overlap the GPU work less."""
+    n = args.n
+    c_h = np.zeros(n * n)
+    L.b2_set_dgemm_method(method, args.slices)
+    ip = lambda v: C.byref(C.c_int(v))
+    one, zero = C.c_double(1.0), C.c_double(0.0)
+
+    def call():
+        L.dgemm_(b"N", b"N", ip(n), ip(n), ip(n), C.byref(one), a_h.ctypes.data, ip(n),
+                 b_h.ctypes.data, ip(n), C.byref(zero), c_h.ctypes.data, ip(n))
+        if L.b2_last_error() != 0:
+            raise RuntimeError(f"dgemm_ failed: {L.b2_last_error()}")
+
+    call()
+    steps = max(2, min(args.steps, 3))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        call()
+    dt = (time.perf_counter() - t0) / steps
+    if dist:
+        dt = max_over_ranks(dt * 1e3, dist, dev) / 1e3
+    L.b2_set_dgemm_method(_lib_fp64(), 0)
+    return {"value": world * 2.0 * n ** 3 / dt / 1e12, "unit": "TFLOPS",
+            "h2d_bytes_per_step": 2 * 8 * n * n, "d2h_bytes_per_step": 8 * n * n,
+            "ms_per_step": dt * 1e3,
+            "note": "drop-in dgemm_ on pageable (malloc'ed) host A, B, C, same call"}
+
+
 def pinned_copy_gbs(pin_src, pin_dst, dev):
     """This box's pinned copy rates (GB/s): host-to-device alone, and
     host-to-device plus device-to-host on two streams at once (bytes of both
@@ -534,12 +566,35 @@ def _lib_fp64():
     return _lib.METHODS["fp64"]
 
 
+def launcher_command(argv, gpus: int, port: int):
+    """torchrun command that runs this script as `gpus` ranks on this node.
+    `--n` is passed on as `--size` (torchrun's own parser would take `--n` for
+    an abbreviation of one of its options)."""
+    fwd = ["--size" if a == "--n" else ("--size=" + a[4:] if a.startswith("--n=") else a)
+           for a in argv]
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={gpus}", "--master-addr", "127.0.0.1", f"--master-port={port}",
+            os.path.abspath(__file__), *fwd]
+
+
+def free_port() -> int:
+    import socket
+
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "RANK" not in os.environ:
+        # asked for N GPUs without a launcher: start the N ranks here (one
+        # process per GPU), never time one replica under an N-GPU label
+        return subprocess.call(launcher_command(sys.argv[1:], args.gpus, free_port()))
     rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", args.gpus if "RANK" in os.environ else 1))
+    world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
-        line = reference_arm(args, rank)
+        line = reference_arm(args, rank, world)
         if line is not None:
             print(json.dumps(line), flush=True)
         return 0

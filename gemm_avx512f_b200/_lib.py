@@ -101,6 +101,10 @@ def lib() -> C.CDLL:
     L.b2_device_error.argtypes = [i]
     L.b2_dgemm_ozaki_noalloc.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, p]
     L.b2_dgemm_ozaki_noalloc.restype = i
+    L.b2_dgemm_ozaki_noalloc_error.argtypes = [i, p]
+    L.b2_dgemm_ozaki_noalloc_error.restype = i
+    L.b2_test_bounded_wait.argtypes = [C.c_longlong, i]
+    L.b2_test_bounded_wait.restype = i
     L.b2_gemm_grouped.argtypes = [i, p, p]
     L.b2_grouped_plan_create.argtypes = [i, p, C.POINTER(C.c_void_p)]
     L.b2_grouped_plan_launch.argtypes = [p, p]

@@ -49,7 +49,7 @@ struct CtxOwner {
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int i = 0; i < WS_COUNT; ++i)
       if (c->ws[i]) cudaFree(c->ws[i]);
-    if (c->derr) cudaFree(c->derr);
+    if (c->derr && !c->derr_host) cudaFree(c->derr);
     if (c->pinned) cudaFreeHost(c->pinned);
     if (c->h2d) cudaStreamSynchronize(c->h2d), cudaStreamDestroy(c->h2d);
     if (c->d2h) cudaStreamSynchronize(c->d2h), cudaStreamDestroy(c->d2h);
@@ -94,7 +94,6 @@ Ctx *ctx() {
   c->cc_major = prop.major;
   c->cc_minor = prop.minor;
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&c->derr, 64) != cudaSuccess || cudaMemset(c->derr, 0, 64) != cudaSuccess ||
       cudaMallocHost(&c->pinned, 4096) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking) != cudaSuccess) {
@@ -120,6 +119,18 @@ Ctx *ctx() {
     (void)cudaGetLastError();
     c->pinned_dev = nullptr;
   }
+  // The kernels' error word: mapped pinned memory at offset 128 when the
+  // device can address it (the host then reads it without a copy after a
+  // synchronisation), else 64 bytes of device memory.
+  if (c->pinned_dev) {
+    c->derr_host = (int *)((uint8_t *)c->pinned + 128);
+    c->derr = (int *)((uint8_t *)c->pinned_dev + 128);
+    *c->derr_host = 0;
+  } else if (cudaMalloc(&c->derr, 64) != cudaSuccess || cudaMemset(c->derr, 0, 64) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete c;
+    return nullptr;
+  }
   c->dgemm_method = method_from_env(getenv("B2_METHOD"), B2_METHOD_FP64);
   c->sgemm_method = method_from_env(getenv("B2_SGEMM_METHOD"), B2_METHOD_FP32);
   if (const char *s = getenv("B2_SLICES")) c->dgemm_slices = atoi(s);
@@ -135,6 +146,20 @@ Ctx *ctx() {
     }
   }
   return c;
+}
+
+int take_device_error(Ctx *c, int st) {
+  int v = 0;
+  if (c->derr_host) {
+    v = *(volatile int *)c->derr_host;
+    if (v) *(volatile int *)c->derr_host = 0;
+  } else if (cudaMemcpy(&v, c->derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return st == B2_OK ? B2_ERR_CUDA : st;
+  } else if (v && cudaMemset(c->derr, 0, sizeof(int)) != cudaSuccess) {
+    (void)cudaGetLastError();
+  }
+  return (st == B2_OK && v) ? B2_ERR_TIMEOUT : st;
 }
 
 void *workspace(Ctx *c, int slot, size_t bytes) {
@@ -534,6 +559,7 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = cuda_fail(e, "stream sync");
   }
+  st = take_device_error(c, st);
   set_status(st);
   return st;
 }
@@ -590,6 +616,7 @@ static void gemm3m_dropin(const char *transa, const char *transb, const int *m, 
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = cuda_fail(e, "stream sync");
   }
+  st = take_device_error(cx, st);
   set_status(st);
 }
 
@@ -954,6 +981,7 @@ void dtrsm_(const char *side, const char *uplo, const char *transa, const char *
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = cuda_fail(e, "stream sync");
   }
+  st = take_device_error(cx, st);
   set_status(st);
 }
 
@@ -1143,15 +1171,31 @@ int b2_set_arg_mode(int mode) {
 int b2_device_error(int clear) {
   Ctx *c = ctx();
   if (!c) return B2_ERR_NO_DEVICE;
-  int v = 0;
-  if (cudaMemcpyAsync(c->pinned, c->derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
-      cudaStreamSynchronize(c->stream) != cudaSuccess) {
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     (void)cudaGetLastError();
     return B2_ERR_CUDA;
   }
-  v = *(int *)c->pinned;
-  if (clear) cudaMemsetAsync(c->derr, 0, 64, c->stream), cudaStreamSynchronize(c->stream);
+  int v = 0;
+  if (c->derr_host) {
+    v = *(volatile int *)c->derr_host;
+    if (clear) *(volatile int *)c->derr_host = 0;
+    return v;
+  }
+  if (cudaMemcpy(&v, c->derr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return B2_ERR_CUDA;
+  }
+  if (clear && cudaMemset(c->derr, 0, 64) != cudaSuccess) (void)cudaGetLastError();
   return v;
+}
+
+int b2_test_bounded_wait(long long wait_ns, int withhold_launches) {
+  if (withhold_launches < 0) return B2_ERR_ARG;
+  unsigned long long w = wait_ns <= 0 ? umma_default_wait_ns() : (unsigned long long)wait_ns;
+  if (w < 100000ull) w = 100000ull;               // 0.1 ms
+  if (w > 10000000000ull) w = 10000000000ull;     // 10 s
+  umma_set_wait(w, withhold_launches);
+  return B2_OK;
 }
 
 }  // extern "C"

@@ -43,7 +43,9 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   void *ws[WS_COUNT] = {};
   size_t ws_bytes[WS_COUNT] = {};
-  int *derr = nullptr;        // device error word
+  int *derr = nullptr;        // error word the kernels write (device address)
+  int *derr_host = nullptr;   // the same word seen from the host when it is mapped
+                              // pinned memory (then no copy is needed to read it)
   void *pinned = nullptr;     // small pinned scratch for host reads
   void *pinned_dev = nullptr; // its device address (kernels store to it directly), or null
   int dgemm_method = B2_METHOD_FP64;
@@ -60,6 +62,13 @@ struct Ctx {
 };
 
 Ctx *ctx();                          // initialises on first use; nullptr if no device
+// Wait limit of the tensor-core engines' bounded waits and the number of
+// launches that withhold their first copy (test hook; umma.cu).
+unsigned long long umma_default_wait_ns();
+void umma_set_wait(unsigned long long wait_ns, int withhold_launches);
+// Reads (and clears) the error word after the caller's stream has been
+// synchronised: B2_ERR_TIMEOUT when a bounded device wait gave up, else st.
+int take_device_error(Ctx *c, int st);
 void *workspace(Ctx *c, int slot, size_t bytes);  // nullptr on allocation failure
 cudaStream_t pick_stream(Ctx *c, void *user_stream);
 

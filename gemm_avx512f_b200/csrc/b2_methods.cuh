@@ -35,6 +35,14 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                 const double *B, int ldb, double beta, double *C, int ldc, int slices,
                 cudaStream_t s);
 int ozaki_auto_moduli(int k);
+// The allocation-free Ozaki DGEMM on a caller-provided scratch area (base,
+// cap bytes, 256-byte aligned; word 0 is the kernels' error word): scratch
+// bytes one call needs, and the call itself (B2_ERR_ARG when it does not fit).
+size_t ozaki_noalloc_bytes(int m, int n, int k, int s);
+int ozaki_noalloc_run(unsigned char *base, size_t cap, int dev, int sm_count, char transa,
+                      char transb, int m, int n, int k, double alpha, const double *A, int lda,
+                      const double *B, int ldb, double beta, double *C, int ldc, int slices,
+                      cudaStream_t st);
 void ozaki_set_variant(int v);  // INT8 engine shape of the allocating path (0..4; -1 = default)
 // Host-operand pipeline state of this thread: the next Ozaki DGEMM computes
 // rows [r0, r0 + m) of op(A) for column block j, op(A) being m_full rows whose

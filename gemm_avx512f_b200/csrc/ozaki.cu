@@ -1077,85 +1077,43 @@ extern "C" int b2_ozaki_last_plan(int *out, int n) {
 }
 
 // ---------------------------------------------------------------------------
-// Allocation-free variant of the Ozaki DGEMM.
-//
-// Some callers cannot allocate device memory at call time: code that runs
-// while a CUDA graph is being captured, real-time loops that must not enter
-// the allocator, or processes whose device memory is fully reserved up front
-// by another framework.  For them b2_dgemm_ozaki_noalloc runs the same
-// kernels as b2_dgemm(..., B2_METHOD_OZAKI, ...) but takes every scratch
-// buffer (residue slices, residue products, scaling exponents, the device
-// error word) from the file-scope array below, which the loader reserves once
-// per device when the library is loaded and which stays reserved until exit.
-// It never calls cudaMalloc/cudaFree or any allocating routine, and does not
-// touch the per-thread context (whose first use allocates).
-//
-// Limits and sharing: a call needs
-//   s*(m*kp + n*kp + n*mp) + (m + n)*(4 + 16*chunks) bytes (+ alignment),
-// kp = K rounded up to 16 (K <= 65536), mp = m rounded up to 16, s = moduli,
-// chunks = norm pass K chunks (<= 64); anything above B2_NOALLOC_SCRATCH_BYTES is
-// rejected with B2_ERR_ARG.  All calls on a device share the one array and
-// it keeps the previous call's contents, so calls that overlap on the GPU
-// (different streams, or different host threads) race; serialise them.
-// The first call on each device looks the array's device address up with
-// cudaGetSymbolAddress (the array's name is only a host-side stand-in), so
-// that first call should come before any stream capture.
+// Body of the allocation-free Ozaki DGEMM (the entry point, its static scratch
+// array and the array's set-up live in ozaki_noalloc.cu).  Every scratch
+// buffer is carved out of `base` (cap bytes, 256-byte aligned):
+//   [error word][modulus count][sigma|tau][norm scratch A|B][Y][X][R]
+// The call needs s*(m*kp + n*kp + n*mp) + (m + n)*4 + the norm scratch
+// (24 bytes per row and K chunk) + alignment, kp = K rounded up to 16
+// (K <= 65536), mp = m rounded up to 16; a larger problem is refused with
+// B2_ERR_ARG before anything is launched.  Device pointers only (checked by
+// the caller).  Nothing here allocates.
 // ---------------------------------------------------------------------------
 namespace b2 {
-namespace {
 
-static __device__ __align__(256) unsigned char g_noalloc_scratch[B2_NOALLOC_SCRATCH_BYTES];
-
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::mutex g_noalloc_mu;
-void *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
-
-int noalloc_base(int dev, unsigned char **out) {
-  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return B2_ERR_NO_DEVICE;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return cuda_fail(e, "cudaGetSymbolAddress(noalloc scratch)");
-    g_noalloc_addr[dev] = p;
-  }
-  *out = (unsigned char *)g_noalloc_addr[dev];
-  return B2_OK;
+size_t ozaki_noalloc_bytes(int m, int n, int k, int s) {
+  const long long kp = round_up(k, 16), mp = round_up(m, 16);
+  size_t off = 256;
+  off += round_up((long long)(m + n) * sizeof(int), 256);
+  off += round_up(norm_scratch_bytes(m, k), 256);
+  off += round_up(norm_scratch_bytes(n, k), 256);
+  off += round_up((long long)m * kp * s, 256);
+  off += round_up((long long)n * kp * s, 256);
+  off += round_up((long long)n * mp * s, 256);
+  return off;
 }
 
-}  // namespace
-}  // namespace b2
-
-extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, int k,
-                                      double alpha, const double *A, int lda, const double *B,
-                                      int ldb, double beta, double *C, int ldc, int slices,
-                                      void *stream) {
-  using namespace b2;
-  int info = 0;
-  int rc = check_gemm(transa, transb, m, n, k, lda, ldb, ldc, A, B, C, &info);
-  if (rc != B2_OK) return rc;
-  if (m == 0 || n == 0) return B2_OK;
-  int dev = 0;
-  cudaDeviceProp prop;
-  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return B2_ERR_NO_DEVICE;
-  }
-  if (prop.major < 10) return B2_ERR_NO_DEVICE;
-  cudaStream_t st = (cudaStream_t)stream;
-  if (!is_device_ptr(C) || (k > 0 && alpha != 0.0 && (!is_device_ptr(A) || !is_device_ptr(B))))
-    return B2_ERR_ARG;
-  if (k == 0 || alpha == 0.0) return beta == 1.0 ? B2_OK : scale_matrix_d(m, n, beta, C, ldc, st);
+int ozaki_noalloc_run(unsigned char *base, size_t cap, int dev, int sm_count, char transa,
+                      char transb, int m, int n, int k, double alpha, const double *A, int lda,
+                      const double *B, int ldb, double beta, double *C, int ldc, int slices,
+                      cudaStream_t st) {
   const int s = slices > 0 ? slices : ozaki_auto_moduli(k);
   if (s < 2 || s > OZ_MAX) return B2_ERR_ARG;
-  const int KCH = 1 << 16;
-  if (k > KCH) return B2_ERR_ARG;  // one exact INT32 pass only
+  if (k > (1 << 16)) return B2_ERR_ARG;  // one exact INT32 pass only
+  if (ozaki_noalloc_bytes(m, n, k, s) > cap) return B2_ERR_ARG;
 
   const long long kp = round_up(k, 16), mp = round_up(m, 16);
   const long long planeY = (long long)m * kp, planeX = (long long)n * kp;
   const long long planeR = (long long)n * mp;
   const size_t nsA = norm_scratch_bytes(m, k), nsB = norm_scratch_bytes(n, k);
-  // carve: [error word][sigma|tau][norm scratch A][norm scratch B][Y][X][R]
   size_t off = 256;
   const size_t o_sig = off;
   off += round_up((long long)(m + n) * sizeof(int), 256);
@@ -1168,12 +1126,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   const size_t o_X = off;
   off += round_up(planeX * s, 256);
   const size_t o_R = off;
-  off += round_up(planeR * s, 256);
-  if (off > (size_t)B2_NOALLOC_SCRATCH_BYTES) return B2_ERR_ARG;
 
-  unsigned char *base = nullptr;
-  rc = noalloc_base(dev, &base);
-  if (rc != B2_OK) return rc;
   int *derr = (int *)base;
   int *s_dev = (int *)(base + 64);  // modulus count read by the kernels (set below)
   int *sigA = (int *)(base + o_sig);
@@ -1184,7 +1137,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   // the error word is the only state that must start at zero
   B2_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), st));
 
-  rc = upload_tables(dev, st);
+  int rc = upload_tables(dev, st);
   if (rc != B2_OK) return rc;
   const CrtTable t = make_table(s);
   const bool tA = !(transa == 'N' || transa == 'n');
@@ -1220,11 +1173,13 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, k, m, s, kp, planeY, 256);
   if (rc != B2_OK) return rc;
   ResidueEpi epi{Rb, planeR, (int)mp, n, m, 0};
-  rc = umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, k, s, epi, prop.multiProcessorCount,
-                                            derr, st, "ozaki_i8_gemm");
+  rc = umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, k, s, epi, sm_count, derr, st,
+                                            "ozaki_i8_gemm");
   if (rc != B2_OK) return rc;
-  launch_reconstruct(Rb, planeR, (int)mp, s_dev, s, s, m, n, sigA, tauB, alpha, beta, C, ldc, A, asr, ask, B,
-                     bsk, bsr, k, st);
+  launch_reconstruct(Rb, planeR, (int)mp, s_dev, s, s, m, n, sigA, tauB, alpha, beta, C, ldc, A,
+                     asr, ask, B, bsk, bsr, k, st);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
+
+}  // namespace b2

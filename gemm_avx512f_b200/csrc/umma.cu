@@ -9,6 +9,9 @@
 namespace b2 {
 namespace umma {
 
+std::atomic<unsigned long long> g_wait_ns{B2_WAIT_NS};
+std::atomic<int> g_withhold{0};
+
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
@@ -45,4 +48,11 @@ int make_kmajor_map(CUtensorMap *map, int kind, const void *base, long long kele
 }
 
 }  // namespace umma
+
+unsigned long long umma_default_wait_ns() { return umma::B2_WAIT_NS; }
+void umma_set_wait(unsigned long long wait_ns, int withhold_launches) {
+  umma::g_wait_ns.store(wait_ns);
+  umma::g_withhold.store(withhold_launches);
+}
+
 }  // namespace b2

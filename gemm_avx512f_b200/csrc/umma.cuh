@@ -18,11 +18,13 @@
 // TMEM holds two accumulators (2 x BN columns) so the epilogue of tile i
 // overlaps the MMAs of tile i+1.
 //
-// Every mbarrier wait is bounded (B2_WAIT_NS of wall time from %globaltimer);
-// on expiry the waiter records B2_ERR_TIMEOUT in the device error word and
-// raises a shared abort flag, every role drains and leaves its loop, the
-// in-flight copies and MMAs are waited for (again bounded), TMEM is freed and
-// the kernel returns.  Nothing traps.
+// Every mbarrier wait is bounded (Problem::wait_ns of wall time from
+// %globaltimer, 2 s unless a test shortens it); on expiry the waiter stores
+// B2_ERR_TIMEOUT into the error word (device memory, or host memory mapped
+// into the device so the host reads it without a copy) and raises a shared
+// abort flag, every role leaves its loop, and once all roles have stopped the
+// producer waits (again bounded) for the copies still in flight; TMEM is
+// freed and the kernel returns.  Nothing traps.
 #pragma once
 
 #include <cuda.h>
@@ -43,6 +45,20 @@ constexpr int BM = 128;            // accumulator lanes (X rows) per tile
 constexpr int KBLOCK_BYTES = 128;  // one 128B swizzle atom along K per stage
 constexpr int THREADS = 192;
 constexpr uint64_t B2_WAIT_NS = 2000000000ull;  // 2 s per wait: far above any legal wait
+
+// Wait limit (ns) given to the next launches and the number of launches that
+// withhold their first K-block's TMA loads (a stall made on purpose, used only
+// by the failure-detection tests through b2_test_bounded_wait).
+extern std::atomic<unsigned long long> g_wait_ns;
+extern std::atomic<int> g_withhold;
+// Reads the two settings above for one launch (consumes one withheld launch).
+inline void launch_wait_settings(uint64_t *wait_ns, int *withhold) {
+  *wait_ns = g_wait_ns.load(std::memory_order_relaxed);
+  int w = g_withhold.load(std::memory_order_relaxed);
+  while (w > 0 && !g_withhold.compare_exchange_weak(w, w - 1)) {
+  }
+  *withhold = w > 0 ? 1 : 0;
+}
 
 __host__ __device__ constexpr int elem_bytes(int kind) { return kind == KIND_I8 ? 1 : kind == KIND_BF16 ? 2 : 4; }
 
@@ -75,6 +91,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
 }
+// Completes `bytes` of a phase's expected transaction count without a copy
+// (for copies that were never issued, so that the phase can still complete).
+__device__ __forceinline__ void mbar_complete_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
@@ -90,22 +111,36 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Records a timeout in the error word.  A plain store (every writer stores
+// the same value), so the word may live in mapped host memory.
+__device__ __forceinline__ void record_timeout(int *derr) {
+  *reinterpret_cast<volatile int *>(derr) = (int)B2_ERR_TIMEOUT;
+  __threadfence_system();
+}
+
 // Bounded wait.  Returns false if the wait was abandoned (timeout here or an
-// abort raised by another role); the first timeout records the error.
+// abort raised by another role); a timeout records the error.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
-                                          int *derr) {
+                                          int *derr, uint64_t limit_ns) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = gtimer();
   for (uint32_t it = 1;; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((it & 255u) == 0) {
       if (*abort_flag) return false;
-      if (gtimer() - t0 > B2_WAIT_NS) {
+      if (gtimer() - t0 > limit_ns) {
         *abort_flag = 1;
-        atomicCAS(derr, 0, (int)B2_ERR_TIMEOUT);
+        record_timeout(derr);
         return false;
       }
     }
+  }
+}
+
+// Bounded plain wait (no abort flag, no error): used while draining.
+__device__ __forceinline__ void mbar_wait_drain(uint32_t bar, uint32_t parity, uint64_t limit_ns) {
+  const uint64_t t0 = gtimer();
+  while (!mbar_try_wait(bar, parity) && gtimer() - t0 < limit_ns) {
   }
 }
 
@@ -211,6 +246,9 @@ struct Problem {
   // within three K' blocks and is served by L2.
   int seg_kb;
   unsigned seg_x, seg_y;
+  uint64_t wait_ns;  // limit of every bounded wait
+  int withhold;      // test only: the first fill of each producer posts its
+                     // byte count but issues no copy (the wait for it times out)
 };
 
 template <int BN, int STAGES>
@@ -219,7 +257,8 @@ struct SmemLayout {
   static constexpr int Y_BYTES = BN * KBLOCK_BYTES;
   static constexpr int STAGE_BYTES = X_BYTES + Y_BYTES;
   static constexpr int BAR_OFF = STAGES * STAGE_BYTES;
-  // full[S], empty[S], tfull[2], tempty[2], drain, then tmem address + abort flag
+  // full[S], empty[S], tfull[2], tempty[2], drain, then tmem address (+0),
+  // abort flag (+8) and the CTA pair's odd-CTA fill count (+12)
   static constexpr int BAR_BYTES = (2 * STAGES + 5) * 8;
   static constexpr int TOTAL = BAR_OFF + BAR_BYTES + 16 + 1024;  // + alignment slack
 };
@@ -289,15 +328,13 @@ __global__ void __launch_bounds__(THREADS, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  long issued = 0;  // fills posted by the producer (warp 0, lane 0)
   if (warp == 0) {
     // ------------------------------------------------------ TMA producer
     if (lane == 0) {
-      constexpr int EB = 0;  // silence unused warnings in some instantiations
-      (void)EB;
       const int kcoord = KBLOCK_BYTES / elem_bytes(KIND);
       int stage = 0;
       uint32_t phase = 0;
-      long issued = 0;
       bool ok = true;
       for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x) {
         const int t = u / pr.ksplit, ks = u - t * pr.ksplit;
@@ -305,7 +342,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         tile_coords(pr, t, b, tp, tq);
         const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
         for (int kb = kb0; kb < kb1; ++kb) {
-          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, pr.derr)) { ok = false; break; }
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, pr.derr, pr.wait_ns)) {
+            ok = false;
+            break;
+          }
           const uint32_t sx = base + stage * L::STAGE_BYTES;
           const uint32_t sy = sx + L::X_BYTES;
           mbar_expect_tx(full_bar(stage), L::STAGE_BYTES);
@@ -315,22 +355,12 @@ __global__ void __launch_bounds__(THREADS, 1)
             kx = ((int)((pr.seg_x >> tt) & 1u) * pr.seg_kb + kq) * kcoord;
             ky = ((int)((pr.seg_y >> tt) & 1u) * pr.seg_kb + kq) * kcoord;
           }
-          tma_load_3d(sx, &tmX, full_bar(stage), kx, tp * BM, b);
-          tma_load_3d(sy, &tmY, full_bar(stage), ky, tq * BN, b);
+          if (!(pr.withhold && issued == 0)) {
+            tma_load_3d(sx, &tmX, full_bar(stage), kx, tp * BM, b);
+            tma_load_3d(sy, &tmY, full_bar(stage), ky, tq * BN, b);
+          }
           ++issued;
           if (++stage == STAGES) { stage = 0; phase ^= 1u; }
-        }
-      }
-      if (!ok) {
-        // Abandoned: wait (bounded) until every issued copy has landed so no
-        // TMA writes into shared memory after this CTA retires.
-        long first = issued - STAGES > 0 ? issued - STAGES : 0;
-        for (long i = first; i < issued; ++i) {
-          const int s = (int)(i % STAGES);
-          const uint32_t ph = (uint32_t)((i / STAGES) & 1);
-          const uint64_t t0 = gtimer();
-          while (!mbar_try_wait(full_bar(s), ph) && gtimer() - t0 < B2_WAIT_NS) {
-          }
         }
       }
     }
@@ -347,11 +377,17 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
         const int acc = it & 1;
         const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
-        if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag, pr.derr)) { ok = false; break; }
+        if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag, pr.derr, pr.wait_ns)) {
+          ok = false;
+          break;
+        }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
         for (int kb = kb0; kb < kb1; ++kb) {
-          if (!mbar_wait(full_bar(stage), phase, abort_flag, pr.derr)) { ok = false; break; }
+          if (!mbar_wait(full_bar(stage), phase, abort_flag, pr.derr, pr.wait_ns)) {
+            ok = false;
+            break;
+          }
           tc_fence_after();
           const uint32_t sx = base + stage * L::STAGE_BYTES;
           const uint32_t sy = sx + L::X_BYTES;
@@ -368,9 +404,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       }
       // All MMAs issued so far complete before the drain barrier flips.
       tc_commit(drain_bar);
-      const uint64_t t0 = gtimer();
-      while (!mbar_try_wait(drain_bar, 0) && gtimer() - t0 < B2_WAIT_NS) {
-      }
+      mbar_wait_drain(drain_bar, 0, pr.wait_ns);
     }
   } else {
     // ---------------------------------------------------------- epilogue
@@ -381,7 +415,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       int b, tp, tq;
       tile_coords(pr, t, b, tp, tq);
       const int acc = it & 1;
-      const bool ok = mbar_wait(tfull_bar(acc), (uint32_t)((it >> 1) & 1), abort_flag, pr.derr);
+      const bool ok =
+          mbar_wait(tfull_bar(acc), (uint32_t)((it >> 1) & 1), abort_flag, pr.derr, pr.wait_ns);
       if (!__all_sync(0xffffffffu, ok)) break;  // keep the warp converged for tcgen05.ld
       tc_fence_after();
       const int p = tp * BM + quarter * 32 + lane;
@@ -400,8 +435,20 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 
   tc_fence_before();
-  __syncthreads();
+  __syncthreads();  // every role has left its loop: the abort flag is final
   tc_fence_after();
+  if (warp == 0 && lane == 0 && *abort_flag) {
+    // Abandoned: wait (bounded) until the copies of the newest fill of every
+    // stage have landed (older fills were consumed), so no TMA writes into
+    // shared memory after this CTA retires.  A withheld fill never receives
+    // its bytes; they are completed here so its phase can still flip.
+    const long first = issued - STAGES > 0 ? issued - STAGES : 0;
+    for (long i = first; i < issued; ++i) {
+      const int s = (int)(i % STAGES);
+      if (pr.withhold && i == 0) mbar_complete_tx(full_bar(s), L::STAGE_BYTES);
+      mbar_wait_drain(full_bar(s), (uint32_t)((i / STAGES) & 1), pr.wait_ns);
+    }
+  }
   if (warp == 1) {
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
@@ -509,8 +556,8 @@ __device__ __forceinline__ void tc_mma_pair(uint32_t tmem_d, uint64_t adesc, uin
 // Bounded wait that also raises the peer CTA's abort flag on a timeout.
 __device__ __forceinline__ bool mbar_wait_pair(uint32_t bar, uint32_t parity,
                                                volatile int *abort_flag, uint32_t peer_abort,
-                                               int *derr) {
-  if (mbar_wait(bar, parity, abort_flag, derr)) return true;
+                                               int *derr, uint64_t limit_ns) {
+  if (mbar_wait(bar, parity, abort_flag, derr, limit_ns)) return true;
   st_cluster_u32(peer_abort, 1u);
   return false;
 }
@@ -537,6 +584,9 @@ __global__ void __launch_bounds__(THREADS, 1)
   const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(gbase + L::BAR_OFF + L::BAR_BYTES);
   volatile int *abort_flag = reinterpret_cast<volatile int *>(gbase + L::BAR_OFF + L::BAR_BYTES + 8);
+  // the odd CTA's fill count, stored into the leader's copy of this word
+  volatile uint32_t *odd_fills =
+      reinterpret_cast<volatile uint32_t *>(gbase + L::BAR_OFF + L::BAR_BYTES + 12);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t rank = cluster_rank();
@@ -557,6 +607,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     mbar_init(drain_bar, 1);
     *abort_flag = 0;
+    *odd_fills = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     prefetch_tmap(&tmX);
@@ -574,13 +625,13 @@ __global__ void __launch_bounds__(THREADS, 1)
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
 
+  long issued = 0;  // fills this CTA's producer (warp 0, lane 0) took part in
   if (warp == 0) {
     // ------------------------------------------------------ TMA producer
     if (lane == 0) {
       const int kcoord = KBLOCK_BYTES / elem_bytes(KIND);
       int stage = 0;
       uint32_t phase = 0;
-      long issued = 0;
       bool ok = true;
       for (int t = pair; t < total_tiles && ok; t += npairs) {
         int b, tp, tq;
@@ -588,7 +639,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int xrow = tp * PAIR_BM + (int)rank * BM;
         const int yrow = tq * BN + (int)rank * (BN / 2);
         for (int kb = 0; kb < pr.kblocks; ++kb) {
-          if (!mbar_wait_pair(empty_bar(stage), phase ^ 1u, abort_flag, peer_abort, pr.derr)) {
+          if (!mbar_wait_pair(empty_bar(stage), phase ^ 1u, abort_flag, peer_abort, pr.derr,
+                              pr.wait_ns)) {
             ok = false;
             break;
           }
@@ -596,31 +648,17 @@ __global__ void __launch_bounds__(THREADS, 1)
           const uint32_t sy = sx + L::X_BYTES;
           const uint32_t fb = map_rank(full_bar(stage), 0);
           if (leader) mbar_expect_tx(full_bar(stage), 2 * L::STAGE_BYTES);
-          tma_load_3d_pair(sx, &tmX, fb, kb * kcoord, xrow, b);
-          tma_load_3d_pair(sy, &tmY, fb, kb * kcoord, yrow, b);
+          if (!(leader && pr.withhold && issued == 0)) {
+            tma_load_3d_pair(sx, &tmX, fb, kb * kcoord, xrow, b);
+            tma_load_3d_pair(sy, &tmY, fb, kb * kcoord, yrow, b);
+          }
           ++issued;
           if (++stage == STAGES) { stage = 0; phase ^= 1u; }
         }
       }
-      if (*abort_flag) {
-        if (leader) {
-          // Wait (bounded) until the fills this CTA posted have landed.
-          long first = issued - STAGES > 0 ? issued - STAGES : 0;
-          for (long i = first; i < issued; ++i) {
-            const int s = (int)(i % STAGES);
-            const uint32_t ph = (uint32_t)((i / STAGES) & 1);
-            const uint64_t t0 = gtimer();
-            while (!mbar_try_wait(full_bar(s), ph) && gtimer() - t0 < B2_WAIT_NS) {
-            }
-          }
-        } else {
-          // The odd CTA cannot observe the leader's barrier: give its last
-          // copies a millisecond (they take microseconds) before leaving.
-          const uint64_t t0 = gtimer();
-          while (gtimer() - t0 < 1000000ull) {
-          }
-        }
-      }
+      // The odd CTA's copies complete on the leader's barriers: the leader
+      // needs this count to drain them if the pair is abandoned.
+      if (!leader) st_cluster_u32(map_rank(smem_u32((const void *)odd_fills), 0), (uint32_t)issued);
     }
   } else if (warp == 1) {
     // ------------------------------------------- MMA issuer (leader only)
@@ -633,14 +671,16 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int t = pair; t < total_tiles && ok; t += npairs, ++it) {
         const int acc = it & 1;
         const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
-        if (!mbar_wait_pair(tempty_bar(acc), acc_phase ^ 1u, abort_flag, peer_abort, pr.derr)) {
+        if (!mbar_wait_pair(tempty_bar(acc), acc_phase ^ 1u, abort_flag, peer_abort, pr.derr,
+                            pr.wait_ns)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
         for (int kb = 0; kb < pr.kblocks; ++kb) {
-          if (!mbar_wait_pair(full_bar(stage), phase, abort_flag, peer_abort, pr.derr)) {
+          if (!mbar_wait_pair(full_bar(stage), phase, abort_flag, peer_abort, pr.derr,
+                              pr.wait_ns)) {
             ok = false;
             break;
           }
@@ -659,9 +699,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         tc_commit_pair(tfull_bar(acc), (uint16_t)3);
       }
       tc_commit_pair(drain_bar, (uint16_t)1);
-      const uint64_t t0 = gtimer();
-      while (!mbar_try_wait(drain_bar, 0) && gtimer() - t0 < B2_WAIT_NS) {
-      }
+      mbar_wait_drain(drain_bar, 0, pr.wait_ns);
     }
   } else {
     // ---------------------------------------------------------- epilogue
@@ -672,7 +710,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       tile_coords(pr, t, b, tp, tq);
       const int acc = it & 1;
       const bool ok = mbar_wait_pair(tfull_bar(acc), (uint32_t)((it >> 1) & 1), abort_flag,
-                                     peer_abort, pr.derr);
+                                     peer_abort, pr.derr, pr.wait_ns);
       if (!__all_sync(0xffffffffu, ok)) break;
       tc_fence_after();
       const int p = tp * PAIR_BM + (int)rank * BM + quarter * 32 + lane;
@@ -692,7 +730,32 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   tc_fence_before();
   __syncthreads();
+  // Both CTAs' roles have left their loops: each abort flag is final (a
+  // failed wait in either CTA raised both) and the odd CTA's fill count has
+  // been stored into the leader.
   cluster_sync();
+  if (leader && warp == 0 && lane == 0 && *abort_flag) {
+    // Abandoned: every copy either CTA issued completes on the leader's full
+    // barriers.  Wait (bounded) for the newest fill of every stage (older
+    // ones were consumed).  A fill posted by only one side gets the other
+    // side's share settled here -- bytes the leader expected but nobody will
+    // copy are completed, a fill only the odd CTA issued gets its arrival --
+    // so every wait below ends as soon as the real copies have landed.
+    const long lf = issued, of = (long)*odd_fills;
+    const long hi = lf > of ? lf : of;
+    const long first = hi - STAGES > 0 ? hi - STAGES : 0;
+    for (long i = first; i < hi; ++i) {
+      const int s = (int)(i % STAGES);
+      if (i >= lf) {
+        mbar_expect_tx(full_bar(s), L::STAGE_BYTES);
+      } else {
+        if (pr.withhold && i == 0) mbar_complete_tx(full_bar(s), L::STAGE_BYTES);
+        if (i >= of) mbar_complete_tx(full_bar(s), L::STAGE_BYTES);
+      }
+      mbar_wait_drain(full_bar(s), (uint32_t)((i / STAGES) & 1), pr.wait_ns);
+    }
+  }
+  cluster_sync();  // no CTA of the pair leaves while the leader drains
   tc_fence_after();
   if (warp == 1) {
     __syncwarp();
@@ -727,6 +790,7 @@ int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long lo
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;
   pr.derr = derr;
+  launch_wait_settings(&pr.wait_ns, &pr.withhold);
   // split-K: ranges of ceil(kblocks / ksplit) blocks, their count recomputed so
   // that none is empty (an empty range would leave its accumulator unwritten)
   if (ksplit < 1) ksplit = 1;
@@ -770,6 +834,7 @@ int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, lo
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;
   pr.derr = derr;
+  launch_wait_settings(&pr.wait_ns, &pr.withhold);
   const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch;
   if (total <= 0) return B2_OK;
   auto kern = umma_gemm_pair_kernel<KIND, BN, STAGES, Epi>;

@@ -169,23 +169,36 @@ B2_API int b2_dgemm_multi(int ndev, const int *devices, char transa, char transb
 B2_API int b2_ozaki_last_plan(int *out, int n);
 
 /* Allocation-free INT8 Ozaki DGEMM.  No counterpart in the reference: it is
- * for callers that cannot allocate device memory at call time (code running
- * during CUDA graph capture, real-time loops that must stay out of the
- * allocator, processes whose device memory is reserved up front).  Same
- * contract and result as b2_dgemm(..., B2_METHOD_OZAKI, slices, stream) on
- * device pointers (slices 0 means 15 moduli here: the heavy-tail switch to 16
- * of the allocating path is not made), but all scratch lives in one static device array of
- * B2_NOALLOC_SCRATCH_BYTES per device, reserved when the library loads and
- * held until exit; the call never allocates or frees.  Problems whose scratch
- * exceeds that maximum (about 1200^3 at 15 moduli; K <= 65536) return
- * B2_ERR_ARG.  Every call shares the array, so calls that overlap on the GPU
- * race and must be serialised by the caller.  The first call on a device
- * resolves the array's device address; make it before any stream capture.
- * stream NULL = the legacy default stream. */
+ * for callers that cannot allocate device memory at call time -- a real-time
+ * loop that must stay out of the allocator, or a process whose device memory
+ * another framework reserved up front, where a cudaMalloc during the call
+ * would fail or stall.  Same contract and result as b2_dgemm(...,
+ * B2_METHOD_OZAKI, slices, stream) on device pointers (slices 0 means 15
+ * moduli here: the heavy-tail switch to 16 of the allocating path is not
+ * made), but all scratch lives in one static device array of
+ * B2_NOALLOC_SCRATCH_BYTES per device, and the call never allocates or frees.
+ * The array sits in its own device module: under lazy module loading (the
+ * CUDA default) it is reserved on a device at the first call there and held
+ * until the process exits; processes that never call this entry point do not
+ * pay for it.  Limit: problems whose scratch exceeds the array -- square ones
+ * above n = 1200 at 15 moduli (1161 at 16), or K > 65536 -- return
+ * B2_ERR_ARG without touching C.  Every call on a device shares the array and
+ * it keeps the last call's contents, so calls that overlap on the GPU race
+ * and must be serialised by the caller.  The first call on a device resolves
+ * the array's device address and uploads constant tables (synchronising its
+ * stream); make it before any stream capture.  The status comes back only as
+ * the return value (b2_last_error() is not updated); a bounded device wait
+ * that gave up is read with b2_dgemm_ozaki_noalloc_error.  stream NULL = the
+ * legacy default stream. */
 #define B2_NOALLOC_SCRATCH_BYTES (64ull << 20)
 B2_API int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, int k, double alpha,
                                   const double *A, int lda, const double *B, int ldb,
                                   double beta, double *C, int ldc, int slices, void *stream);
+/* Error word of the last b2_dgemm_ozaki_noalloc on the current device (kept
+ * in its static array; allocation-free): B2_ERR_TIMEOUT when a bounded device
+ * wait of that call gave up, else 0.  Synchronises `stream`; clear resets the
+ * word.  No counterpart in the reference. */
+B2_API int b2_dgemm_ozaki_noalloc_error(int clear, void *stream);
 
 /* Same contract as sgemm_ (src/gemm_driver.c:116) on device memory. */
 B2_API int b2_sgemm(char transa, char transb, int m, int n, int k, float alpha, const float *A,
@@ -292,10 +305,24 @@ B2_API int b2_dgemm_error(char transa, char transb, int m, int n, int k, double 
                    const double *C0, const double *C, int ldc, double *normwise,
                    double *maxelem, void *stream);
 
-/* Device-side error word: non-zero after a bounded wait inside a kernel gave
- * up (B2_ERR_TIMEOUT).  Reading it synchronizes the library stream; clear
- * resets it. */
+/* Device-side error word of this thread's context: B2_ERR_TIMEOUT after a
+ * bounded wait inside one of its kernels gave up (the reference's own waits
+ * spin forever, src/gemm_driver.c:21-31).  The synchronous drop-in symbols
+ * read and clear it themselves after their final synchronisation and report
+ * B2_ERR_TIMEOUT through b2_last_error(); the asynchronous b2_* calls cannot
+ * know at return, so after synchronising their stream call this.  Reading it
+ * synchronizes the library stream; clear resets it. */
 B2_API int b2_device_error(int clear);
+
+/* Test hook of the failure detection: every later tensor-core launch (the
+ * tcgen05 engines of the Ozaki, split-SGEMM and 3M paths) gives up a wait
+ * after wait_ns nanoseconds instead of 2 s (wait_ns <= 0 restores 2 s; the
+ * value is clamped to [0.1 ms, 10 s]), and the next withhold_launches
+ * launches post their first K-block's byte count without issuing its copy,
+ * so that the wait for it runs out: the kernel records B2_ERR_TIMEOUT, drains
+ * and returns, and the call reports the timeout.  Nothing faults or hangs;
+ * results of a withheld launch are invalid.  Process-wide. */
+B2_API int b2_test_bounded_wait(long long wait_ns, int withhold_launches);
 
 
 /* ------------------------------------------------------------------------ */

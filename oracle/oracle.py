@@ -30,12 +30,21 @@ _lib = None
 _ref = {}
 
 
+def reference_dir() -> str | None:
+    """The reference's source tree: $B2_REFERENCE_DIR, else a directory named
+    ``reference`` beside this repository's root, when it exists; None
+    otherwise (then only the prebuilt _ref/ files, if any, are used)."""
+    cand = os.environ.get("B2_REFERENCE_DIR") or os.path.join(
+        os.path.dirname(os.path.dirname(HERE)), "reference")
+    return cand if os.path.isdir(cand) else None
+
+
 def build(reference: str | None = None, quiet: bool = True) -> None:
     """Compile liboracle.so and, when the reference sources exist, _ref/."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=out, stderr=out)
-    ref = reference or "/root/reference"
-    if os.path.isdir(ref):
+    ref = reference or reference_dir()
+    if ref and os.path.isdir(ref):
         subprocess.run(["make", "-C", HERE, "ref", f"REF={ref}"], check=True, stdout=out,
                        stderr=out)
 
@@ -113,10 +122,15 @@ def gemm_dd(transa, transb, m, n, k, alpha, a, b, beta, c0):
 
 
 def ref_gemm(transa, transb, m, n, k, alpha, a, b, beta, c, which="main"):
-    """The reference's own dgemm_/sgemm_ (Fortran ABI, all by pointer)."""
+    """The reference's own dgemm_/sgemm_ (Fortran ABI, all by pointer):
+    which = "main" (src/gemm_driver.c:116), "oblike" (OpenBLAS-like dgemm.c:484 /
+    sgemm.c:579), "8x8opt" / "8x8std" (kernel_avx512_opt8x8.c:821 /
+    kernel_avx512_standard8x8.c:843, serial, FP64)."""
     dbl = c.dtype == np.float64
     if which == "main":
         fn = ref_lib("DGEMM.so").dgemm_ if dbl else ref_lib("SGEMM.so").sgemm_
+    elif which in ("8x8opt", "8x8std"):  # kernel_avx512_{opt,standard}8x8.c:821/843 (FP64 only)
+        fn = ref_lib("dgemm_8x8_opt.so" if which == "8x8opt" else "dgemm_8x8_std.so").dgemm_
     else:
         fn = ref_lib("oblike_dgemm.so").dgemm_ if dbl else ref_lib("oblike_sgemm.so").SGEMM_
     ct = C.c_double if dbl else C.c_float

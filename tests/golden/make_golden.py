@@ -1,7 +1,7 @@
 """Generate golden vectors by running the REFERENCE itself (oracle/_ref/*.so,
 compiled from the wjc404/GEMM_AVX512F sources by oracle/Makefile).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture.npz ...]
 
 Writes small .npz fixtures next to this script.  Each holds the seeded inputs
 and the reference's outputs, so the oracle restatement and the GPU path can be
@@ -46,6 +46,39 @@ def gemm_cases(dtype, seed):
                 out[key + "_a"], out[key + "_b"] = a, b
                 out[key + "_c"], out[key + "_out"] = c, cout
                 idx += 1
+    out["count"] = np.array(idx)
+    return out
+
+
+def gemm8x8_cases(seed):
+    """The two 8x8 DGEMM files' own serial dgemm_ drivers (kernel_avx512_opt8x8.c:821,
+    kernel_avx512_standard8x8.c:843): 8-row A panels (dgemm_tcopy_8 /
+    dgemm_ncopy_8, :749/:775) and 8-column B panels, K blocks of 168 (opt) or
+    128 (standard), M blocks of 384 / 512; shapes cover ragged panels and
+    several K and M blocks, all four trans combinations."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    idx = 0
+    shapes = [(1, 1, 1), (7, 5, 3), (13, 17, 29), (17, 9, 170), (9, 10, 260), (389, 2, 16)]
+    for which in ("8x8opt", "8x8std"):
+        for (m, n, k) in shapes:
+            for ta in "NT":
+                for tb in "NT":
+                    al, be = ALPHA_BETA[idx % len(ALPHA_BETA)]
+                    ar, ac = (m, k) if ta == "N" else (k, m)
+                    br, bc = (k, n) if tb == "N" else (n, k)
+                    a = np.asfortranarray(rng.uniform(-1, 1, (ar + 3, ac)))
+                    b = np.asfortranarray(rng.uniform(-1, 1, (br + 2, bc)))
+                    c = np.asfortranarray(rng.uniform(-1, 1, (m + 1, n)))
+                    cout = c.copy(order="F")
+                    O.ref_gemm(ta, tb, m, n, k, al, a[:ar], b[:br], be, cout[:m], which=which)
+                    key = f"e{idx}"
+                    out[key + "_meta"] = np.array([m, n, k, ord(ta), ord(tb)], dtype=np.int64)
+                    out[key + "_kind"] = np.array(which)
+                    out[key + "_ab"] = np.array([al, be])
+                    out[key + "_a"], out[key + "_b"] = a, b
+                    out[key + "_c"], out[key + "_out"] = c, cout
+                    idx += 1
     out["count"] = np.array(idx)
     return out
 
@@ -146,14 +179,23 @@ def gemm_kernel_cases(seed):
     return out
 
 
+FIXTURES = {
+    "dgemm_ref.npz": lambda: gemm_cases(np.float64, 11),
+    "sgemm_ref.npz": lambda: gemm_cases(np.float32, 12),
+    "trsm_kernels_ref.npz": lambda: trsm_cases(13),
+    "zgemm3m_kernel_ref.npz": lambda: gemm3m_kernel_cases(14),
+    "gemm_kernels_ref.npz": lambda: gemm_kernel_cases(15),
+    "dgemm_8x8_ref.npz": lambda: gemm8x8_cases(16),
+}
+
+
 def main():
+    """Writes every fixture, or only those named on the command line."""
     if not (O.ref_available("DGEMM.so") and O.host_has_avx512f()):
         raise SystemExit("reference libraries not built or host lacks AVX-512F")
-    np.savez_compressed(os.path.join(HERE, "dgemm_ref.npz"), **gemm_cases(np.float64, 11))
-    np.savez_compressed(os.path.join(HERE, "sgemm_ref.npz"), **gemm_cases(np.float32, 12))
-    np.savez_compressed(os.path.join(HERE, "trsm_kernels_ref.npz"), **trsm_cases(13))
-    np.savez_compressed(os.path.join(HERE, "zgemm3m_kernel_ref.npz"), **gemm3m_kernel_cases(14))
-    np.savez_compressed(os.path.join(HERE, "gemm_kernels_ref.npz"), **gemm_kernel_cases(15))
+    names = [a for a in sys.argv[1:] if a in FIXTURES] or list(FIXTURES)
+    for name in names:
+        np.savez_compressed(os.path.join(HERE, name), **FIXTURES[name]())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

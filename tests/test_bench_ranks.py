@@ -57,3 +57,29 @@ def test_reference_arm_does_no_work_off_rank_zero():
     import bench
 
     assert bench.reference_arm(None, 1) is None  # returns before reading any argument
+
+
+def test_gpus_flag_without_a_launcher_starts_that_many_ranks():
+    """`python bench.py --gpus 2` with no RANK in the environment must run two
+    ranks (it relaunches itself under torch.distributed.run), never one replica
+    under a two-GPU label.  Checked on the reference arm, which needs no GPU:
+    rank 0 prints one line whose n_gpus is the launched world size."""
+    import json
+    import subprocess
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    cmd = bench.launcher_command(["--gpus", "2"], 2, 12345)
+    assert "--nproc-per-node=2" in cmd and "127.0.0.1" in cmd and cmd[-2:] == ["--gpus", "2"]
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    env["OMP_NUM_THREADS"] = "2"
+    res = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2",
+                          "--impl", "reference", "--n", "192", "--steps", "1", "--warmup", "0",
+                          "--cpu-seconds", "0.05"], capture_output=True, text=True, env=env,
+                         timeout=240, cwd=ROOT)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, res.stdout
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2

@@ -46,6 +46,30 @@ def test_dgemm_dropin_host_parity(cuda, m, n, k, ta, tb):
         assert e <= TOL, (m, n, k, ta, tb, al, be, e)
 
 
+@pytest.mark.parametrize("method", ["fp64", "ozaki"])
+def test_dgemm_dropin_matches_8x8_reference_drivers(cuda, method):
+    """Golden outputs of the 8x8 files' own dgemm_ drivers
+    (kernel_avx512_opt8x8.c:821, kernel_avx512_standard8x8.c:843)."""
+    z = np.load(os.path.join(GOLD, "dgemm_8x8_ref.npz"))
+    u = np.finfo(np.float64).eps / 2
+    blas.set_dgemm_method(method, 0)
+    try:
+        for i in range(int(z["count"])):
+            m, n, k, ta, tb = (int(v) for v in z[f"e{i}_meta"])
+            ta, tb = chr(ta), chr(tb)
+            al, be = (float(v) for v in z[f"e{i}_ab"])
+            a, b, c, out = z[f"e{i}_a"], z[f"e{i}_b"], z[f"e{i}_c"], z[f"e{i}_out"]
+            ar = m if ta == "N" else k
+            br = k if tb == "N" else n
+            got = np.asfortranarray(c.copy())
+            blas.dgemm(ta, tb, m, n, k, al, a, a.shape[0], b, b.shape[0], be, got, got.shape[0])
+            assert np.array_equal(got[m:], c[m:]), "padding rows of C were written"
+            e = normalized(got[:m], out[:m], k, a[:ar], b[:br], u)
+            assert e <= TOL, (str(z[f"e{i}_kind"]), m, n, k, ta, tb, e)
+    finally:
+        blas.set_dgemm_method("fp64", 0)
+
+
 @pytest.mark.parametrize("method,plant_nan", [("fp64", True), ("ozaki", True), ("fp64", False),
                                               ("ozaki", False)])
 def test_dgemm_dropin_pipelined_host_operands(cuda, method, plant_nan):

@@ -58,6 +58,45 @@ def test_oracle_gemm_matches_reference_bitexact(dtype):
                 assert np.array_equal(c1, c2)
 
 
+def _gemm8x8_golden():
+    z = np.load(os.path.join(GOLD, "dgemm_8x8_ref.npz"))
+    for i in range(int(z["count"])):
+        m, n, k, ta, tb = (int(v) for v in z[f"e{i}_meta"])
+        al, be = z[f"e{i}_ab"]
+        yield (str(z[f"e{i}_kind"]), m, n, k, chr(ta), chr(tb), float(al), float(be),
+               z[f"e{i}_a"], z[f"e{i}_b"], z[f"e{i}_c"], z[f"e{i}_out"])
+
+
+def test_oracle_gemm_matches_8x8_reference_drivers():
+    """The 8x8 files' own dgemm_ (kernel_avx512_opt8x8.c:821, _standard8x8.c:843)
+    block K by 168 / 128 and M by 384 / 512 and fold alpha into the kernel,
+    so they agree with the main driver's restatement to rounding only:
+    ||C - C_ref||_F / (K u ||A||_F ||B||_F) <= 8, padding rows untouched."""
+    u = 2.0 ** -53
+    kinds = set()
+    for (kind, m, n, k, ta, tb, al, be, a, b, c, out) in _gemm8x8_golden():
+        ar = m if ta == "N" else k
+        br = k if tb == "N" else n
+        got = np.asfortranarray(c.copy())
+        O.gemm(ta, tb, m, n, k, al, a[:ar], b[:br], be, got[:m])
+        assert np.array_equal(got[m:], out[m:])
+        den = max(k, 1) * u * np.linalg.norm(a[:ar]) * np.linalg.norm(b[:br])
+        assert np.linalg.norm(got[:m] - out[:m]) / den <= 8, (kind, m, n, k, ta, tb)
+        kinds.add(kind)
+    assert kinds == {"8x8opt", "8x8std"}
+
+
+@pytest.mark.skipif(not (O.ref_available("dgemm_8x8_opt.so") and O.host_has_avx512f()),
+                    reason="8x8 reference drivers not built here or no AVX-512F")
+def test_8x8_golden_regenerates_from_reference():
+    for (kind, m, n, k, ta, tb, al, be, a, b, c, out) in _gemm8x8_golden():
+        ar = m if ta == "N" else k
+        br = k if tb == "N" else n
+        got = np.asfortranarray(c.copy())
+        O.ref_gemm(ta, tb, m, n, k, al, a[:ar], b[:br], be, got[:m], which=kind)
+        assert np.array_equal(got, out), (kind, m, n, k, ta, tb)
+
+
 def test_oracle_beta_zero_keeps_nan_and_alpha_zero_skips():
     a = np.asfortranarray(np.ones((4, 4)))
     c = np.asfortranarray(np.full((4, 4), np.nan))
