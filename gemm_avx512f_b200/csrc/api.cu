@@ -59,6 +59,10 @@ struct CtxOwner {
       if (c->ev_c[i]) cudaEventDestroy(c->ev_c[i]);
     }
     if (c->plan_ev) cudaEventDestroy(c->plan_ev);
+    for (int i = 0; i < Ctx::OZ_EVENTS; ++i)
+      if (c->oz_ev[i]) cudaEventDestroy(c->oz_ev[i]);
+    if (c->oz_gemm) cudaStreamSynchronize(c->oz_gemm), cudaStreamDestroy(c->oz_gemm);
+    if (c->oz_aux) cudaStreamSynchronize(c->oz_aux), cudaStreamDestroy(c->oz_aux);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
   }
@@ -146,6 +150,32 @@ Ctx *ctx() {
     }
   }
   return c;
+}
+
+bool ozaki_overlap_streams(Ctx *c) {
+  if (c->oz_gemm && c->oz_aux && c->oz_ev[Ctx::OZ_EVENTS - 1]) return true;
+  int lo = 0, hi = 0;
+  if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) {
+    (void)cudaGetLastError();
+    lo = hi = 0;
+  }
+  if (!c->oz_gemm && cudaStreamCreateWithPriority(&c->oz_gemm, cudaStreamNonBlocking, hi) != cudaSuccess) {
+    (void)cudaGetLastError();
+    c->oz_gemm = nullptr;
+    return false;
+  }
+  if (!c->oz_aux && cudaStreamCreateWithPriority(&c->oz_aux, cudaStreamNonBlocking, lo) != cudaSuccess) {
+    (void)cudaGetLastError();
+    c->oz_aux = nullptr;
+    return false;
+  }
+  for (int i = 0; i < Ctx::OZ_EVENTS; ++i)
+    if (!c->oz_ev[i] && cudaEventCreateWithFlags(&c->oz_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      (void)cudaGetLastError();
+      c->oz_ev[i] = nullptr;
+      return false;
+    }
+  return true;
 }
 
 int take_device_error(Ctx *c, int st) {

@@ -59,7 +59,16 @@ struct Ctx {
   cudaStream_t h2d = nullptr, d2h = nullptr;
   cudaEvent_t ev_in[PIPE_EVENTS] = {}, ev_done[PIPE_EVENTS] = {}, ev_c[PIPE_EVENTS] = {};
   cudaEvent_t plan_ev = nullptr;  // marks the host store of the last Ozaki modulus count
+  // Overlapped Ozaki schedule (created at its first use): the INT8 GEMMs run
+  // on a high-priority stream while the slicing and reconstruction of other
+  // column blocks run beside them on an auxiliary stream.
+  static constexpr int OZ_EVENTS = 2 * 16 + 3;  // per block: sliced, multiplied; fork, 2 joins
+  cudaStream_t oz_gemm = nullptr, oz_aux = nullptr;
+  cudaEvent_t oz_ev[OZ_EVENTS] = {};
 };
+// The two streams and the events of the overlapped Ozaki schedule (false when
+// they cannot be created; the caller then runs the plain schedule).
+bool ozaki_overlap_streams(Ctx *c);
 
 Ctx *ctx();                          // initialises on first use; nullptr if no device
 // Wait limit of the tensor-core engines' bounded waits and the number of

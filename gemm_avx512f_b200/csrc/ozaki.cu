@@ -12,10 +12,10 @@
 //     A'_ik = trunc(a_ik 2^sigma_i), B'_kj = trunc(b_kj 2^tau_j).  By
 //     Cauchy-Schwarz |(A'B')_ij| <= 2^2H <= P/4, where P = m_1 ... m_s is the
 //     product of s pairwise-coprime moduli <= 256.
-//  2. Residue slices.  For every modulus, A' mod m and B' mod m in symmetric
-//     form fit in int8; each slice product (A' mod m)(B' mod m) is an exact
-//     INT32 tcgen05 GEMM (|sum| <= K 2^14 < 2^31 for K < 2^17; longer K is cut
-//     into chunks whose residues are added mod m).  The GEMM epilogue keeps only
+//  2. Residue slices.  For every modulus, A' mod m and B' mod m in [0, m)
+//     fit in uint8; each slice product (A' mod m)(B' mod m) is an exact
+//     INT32 tcgen05 GEMM on unsigned 8-bit operands (sum < K 2^16 < 2^31 for
+//     K <= 32768; longer K is cut into passes whose residues are added mod m).  The GEMM epilogue keeps only
 //     the product mod m (one byte per element per modulus).
 //  3. Reconstruction.  The integer C' = A'B' is the unique value in (-P/2, P/2)
 //     with the s residues (Chinese remainder theorem); it is rebuilt exactly in
@@ -42,6 +42,9 @@ namespace b2 {
 namespace {
 
 constexpr int OZ_MAX = 16;
+// K per exact INT32 pass: residues are below 256, so K products stay below
+// 32768 * 255^2 < 2^31; longer K is cut into passes whose residues add mod m.
+constexpr int OZ_KCHUNK = 1 << 15;
 // Pairwise-coprime moduli <= 256 (distinct prime factors), largest first.
 constexpr int kModuli[OZ_MAX] = {256, 255, 253, 251, 247, 241, 239, 233,
                                  229, 227, 223, 217, 211, 199, 197, 193};
@@ -75,10 +78,8 @@ constexpr bool moduli_agree() {
 static_assert(moduli_agree(), "mod_at must list kModuli in order");
 
 // Epilogue constants, indexed by the batch (= modulus) of a GEMM tile:
-// m, bias = m * ceil(2^30 / m) (makes any |d| <= 2^30 non-negative without
-// changing d mod m) and the exact Barrett multiplier ceil(2^39 / m).
+// m and the exact Barrett multiplier ceil(2^39 / m).
 __constant__ unsigned c_mod[OZ_MAX];
-__constant__ unsigned c_ebias[OZ_MAX];
 __constant__ unsigned c_m39[OZ_MAX];
 // CRT tables for every modulus count s = 0..OZ_MAX (index s), uploaded once per
 // device so calls with different counts never re-upload or synchronise.
@@ -297,21 +298,43 @@ __device__ int norm_slow_sigma(const double *p, long long sk, int K, int H) {
 // nonzero fast-range row's flatness log2(||x_r||_1 / (sqrt(K) ||x_r||_2)) to
 // stat[0] and the row count to stat[1] (the modulus-count statistic; about
 // -0.2 for uniform rows, far below -2 when a few elements carry the norm).
-__global__ void norm_finalize_kernel(const double *__restrict__ pmax,
-                                     const double *__restrict__ pssq,
-                                     const double *__restrict__ pl1, int R, int chunks, int H,
-                                     int *__restrict__ sigma, const double *__restrict__ X,
-                                     long long sr, long long sk, int K, double *stat) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double flat = 0.0, cnt = 0.0;
+// Block: 32 rows (lane = row) x 8 warps; warp w sums the chunks c = w mod 8,
+// the eight partial sums are added in warp order (the result does not depend
+// on scheduling), and warp 0 finishes the rows.
+constexpr int FIN_WARPS = 8;
+__global__ void __launch_bounds__(32 * FIN_WARPS)
+    norm_finalize_kernel(const double *__restrict__ pmax, const double *__restrict__ pssq,
+                         const double *__restrict__ pl1, int R, int chunks, int H,
+                         int *__restrict__ sigma, const double *__restrict__ X, long long sr,
+                         long long sk, int K, double *stat) {
+  __shared__ double part[3][FIN_WARPS][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r = blockIdx.x * 32 + lane;
+  double mx = 0.0, ss = 0.0, l1 = 0.0;
   if (r < R) {
-    double mx = 0.0, ss = 0.0, l1 = 0.0;
-#pragma unroll 8
-    for (int c = 0; c < chunks; ++c) {
+#pragma unroll 4
+    for (int c = warp; c < chunks; c += FIN_WARPS) {
       mx = fmax(mx, pmax[(long long)c * R + r]);
       ss += pssq[(long long)c * R + r];
       l1 += pl1[(long long)c * R + r];
     }
+  }
+  part[0][warp][lane] = mx;
+  part[1][warp][lane] = ss;
+  part[2][warp][lane] = l1;
+  __syncthreads();
+  if (warp != 0) return;
+  mx = part[0][0][lane];
+  ss = part[1][0][lane];
+  l1 = part[2][0][lane];
+#pragma unroll
+  for (int w = 1; w < FIN_WARPS; ++w) {
+    mx = fmax(mx, part[0][w][lane]);
+    ss += part[1][w][lane];
+    l1 += part[2][w][lane];
+  }
+  double flat = 0.0, cnt = 0.0;
+  if (r < R) {
     if (mx == 0.0 && ss == 0.0) {
       sigma[r] = 0;
     } else if (isfinite(ss) && mx >= 0x1p-480 && mx <= 0x1p480) {
@@ -324,12 +347,12 @@ __global__ void norm_finalize_kernel(const double *__restrict__ pmax,
       sigma[r] = norm_slow_sigma(X + (long long)r * sr, sk, K, H);
     }
   }
-  if (stat) {  // every lane of every warp reaches this point (no early return)
+  if (stat) {  // every lane of warp 0 reaches this point
     for (int o = 16; o > 0; o >>= 1) {
       flat += __shfl_down_sync(0xffffffffu, flat, o);
       cnt += __shfl_down_sync(0xffffffffu, cnt, o);
     }
-    if ((threadIdx.x & 31) == 0 && cnt > 0.0) {
+    if (lane == 0 && cnt > 0.0) {
       atomicAdd(stat, flat);
       atomicAdd(stat + 1, cnt);
     }
@@ -366,60 +389,69 @@ __global__ void ozaki_decide_kernel(const double *statA, const double *statB, in
 }
 
 // --------------------------------------------------------- residue slices --
-// u = x + 2^62 in [0, 2^63) is split into 21-bit limbs c0, c1, c2 (< 2^21).
-// For modulus m with h = floor(m/2):
-//   sh = c0 + c1 (2^21 mod m) + c2 (2^42 mod m) + ((-2^62 mod m) + h)
-// is congruent to x + h, and sh <= (2^21 - 1) 511 + 383 < 2^30.  Then
-// q = floor(sh * ceil(2^38/m) / 2^38) is exactly floor(sh/m): with
-// ceil(2^38/m) = 2^38/m + d, 0 <= d < 1, the excess sh d / 2^38 < 2^-8 <= 1/m
-// cannot carry the fraction of sh/m past the next integer.  sh - q m lies in
-// [0, m), so sh - q m - h is the symmetric residue of x, in [-h, m-1-h]
-// (int8 for every modulus <= 256).  Six integer operations per modulus.
-struct SliceConst {
-  unsigned m, h, k21, k42, offh, m38;
+// Unsigned residues from byte dot products.  u = x + 2^62 lies in [1, 2^63)
+// for |x| < 2^62; its eight bytes b_0..b_7 are its two 32-bit words.  For
+// modulus m,
+//   sh = sum_j b_j (2^(8j) mod m) + ((m - 2^62 mod m) mod m)
+// is congruent to x modulo m and below 8*255*255 + 255 < 2^19, so two dp4a
+// instructions form it (the constant rides in the accumulator).  Then
+// q = floor(sh * ceil(2^32/m) / 2^32) is exactly floor(sh/m): with
+// ceil(2^32/m) = 2^32/m + d, 0 <= d < 1, the excess sh d / 2^32 < 2^-13 is
+// below 1/m and cannot carry the fraction of sh/m (at most 1 - 1/m) past the
+// next integer.  r = sh - q m in [0, m) is the residue, one byte (uint8 for
+// every modulus <= 256).  Four integer instructions per modulus, no shifts.
+struct ResConst {
+  unsigned lo, hi, off, mul, m;
 };
-__host__ __device__ constexpr SliceConst slice_const(int i) {
-  return SliceConst{mod_at(i), mod_at(i) >> 1, (1u << 21) % mod_at(i),
-                    (unsigned)((1ull << 42) % mod_at(i)),
-                    (unsigned)((mod_at(i) - (1ull << 62) % mod_at(i)) % mod_at(i) + (mod_at(i) >> 1)),
-                    (unsigned)(((1ull << 38) + mod_at(i) - 1) / mod_at(i))};
+__host__ __device__ constexpr unsigned pow2_mod(int e, unsigned m) {
+  return (unsigned)((1ull << e) % m);
 }
+__host__ __device__ constexpr unsigned pack4(unsigned a, unsigned b, unsigned c, unsigned d) {
+  return a | (b << 8) | (c << 16) | (d << 24);
+}
+__host__ __device__ constexpr ResConst res_const(int i) {
+  return ResConst{pack4(pow2_mod(0, mod_at(i)), pow2_mod(8, mod_at(i)), pow2_mod(16, mod_at(i)),
+                        pow2_mod(24, mod_at(i))),
+                  pack4(pow2_mod(32, mod_at(i)), pow2_mod(40, mod_at(i)), pow2_mod(48, mod_at(i)),
+                        pow2_mod(56, mod_at(i))),
+                  (mod_at(i) - pow2_mod(62, mod_at(i))) % mod_at(i),
+                  (unsigned)(((1ull << 32) + mod_at(i) - 1) / mod_at(i)), mod_at(i)};
+}
+static_assert(res_const(0).lo == 1u && res_const(0).hi == 0u && res_const(0).mul == (1u << 24),
+              "modulus 256 keeps the low byte");
 
-// Two's-complement byte of the symmetric residue (in the low 8 bits).
 template <int I>
-__device__ __forceinline__ unsigned sym_residue_byte(unsigned c0, unsigned c1, unsigned c2) {
-  constexpr SliceConst K = slice_const(I);
-  const unsigned sh = c0 + c1 * K.k21 + c2 * K.k42 + K.offh;
-  const unsigned q = __umulhi(sh, K.m38) >> 6;
-  return sh - q * K.m - K.h;
+__device__ __forceinline__ unsigned residue_u8(unsigned lo, unsigned hi) {
+  constexpr ResConst K = res_const(I);
+  const unsigned sh = __dp4a(lo, K.lo, __dp4a(hi, K.hi, K.off));
+  return sh - __umulhi(sh, K.mul) * K.m;
 }
 
 // Writes the 8 residue bytes of one thread's elements for modulus I.
 template <int I>
-__device__ __forceinline__ void store_slice(const unsigned (&c0)[8], const unsigned (&c1)[8],
-                                            const unsigned (&c2)[8], int8_t *dst, int nk) {
+__device__ __forceinline__ void store_slice(const unsigned (&lo)[8], const unsigned (&hi)[8],
+                                            uint8_t *dst, int nk) {
   unsigned r[8];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) r[j] = sym_residue_byte<I>(c0[j], c1[j], c2[j]);
-  const unsigned lo = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040),
+  for (int j = 0; j < 8; ++j) r[j] = residue_u8<I>(lo[j], hi[j]);
+  const unsigned w0 = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040),
                                   0x5410);
-  const unsigned hi = __byte_perm(__byte_perm(r[4], r[5], 0x0040), __byte_perm(r[6], r[7], 0x0040),
+  const unsigned w1 = __byte_perm(__byte_perm(r[4], r[5], 0x0040), __byte_perm(r[6], r[7], 0x0040),
                                   0x5410);
   if (nk == 8) {
-    *reinterpret_cast<uint2 *>(dst) = make_uint2(lo, hi);
+    *reinterpret_cast<uint2 *>(dst) = make_uint2(w0, w1);
   } else {
-    for (int j = 0; j < nk; ++j) dst[j] = (int8_t)(r[j] & 0xFFu);
+    for (int j = 0; j < nk; ++j) dst[j] = (uint8_t)r[j];
   }
 }
 
 template <int I>
-__device__ __forceinline__ void store_slices(const unsigned (&c0)[8], const unsigned (&c1)[8],
-                                             const unsigned (&c2)[8], int s, int8_t *dst,
-                                             long long plane, int nk) {
+__device__ __forceinline__ void store_slices(const unsigned (&lo)[8], const unsigned (&hi)[8],
+                                             int s, uint8_t *dst, long long plane, int nk) {
   if constexpr (I < OZ_MAX) {
     if (I >= s) return;
-    store_slice<I>(c0, c1, c2, dst + (long long)I * plane, nk);
-    store_slices<I + 1>(c0, c1, c2, s, dst, plane, nk);
+    store_slice<I>(lo, hi, dst + (long long)I * plane, nk);
+    store_slices<I + 1>(lo, hi, s, dst, plane, nk);
   }
 }
 
@@ -428,14 +460,14 @@ __device__ __forceinline__ double pow2(int e) {  // e in [-1022, 1023]
 }
 
 // Operand viewed as R x K (element (r,k) at X[r*sr + k*sk]); writes s planes
-// out[i][r][k] (row pitch kp bytes, plane pitch plane bytes) of the symmetric
-// residues of trunc(x * 2^sigma_r).  Tile: 32 rows x 64 k, 256 threads, each
+// out[i][r][k] (row pitch kp bytes, plane pitch plane bytes) of the residues
+// of trunc(x * 2^sigma_r) modulo m_i.  Tile: 32 rows x 64 k, 256 threads, each
 // thread 8 consecutive k of one row.
 template <bool ROWCONT>
 __global__ void __launch_bounds__(256)
     slice_kernel(const double *__restrict__ X, long long sr, long long sk, int R, int K,
                  const int *__restrict__ sigma, const int *__restrict__ s_dev,
-                 int8_t *__restrict__ out, long long kp, long long plane) {
+                 uint8_t *__restrict__ out, long long kp, long long plane) {
   __shared__ double tile[32][65];
   const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 32;
   const int tid = threadIdx.x;
@@ -458,17 +490,16 @@ __global__ void __launch_bounds__(256)
   // 2^sigma as two in-range factors (sigma in [H-1024, H+1074])
   const int e1 = dead ? 0 : (sg > 1000 ? 1000 : (sg < -1000 ? -1000 : sg));
   const double f1 = pow2(e1), f2 = pow2(dead ? 0 : sg - e1);
-  unsigned c0[8], c1[8], c2[8];
+  unsigned lo[8], hi[8];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     const double v = dead ? 0.0 : (tile[rr][kg + j] * f1) * f2;
     const unsigned long long u = (unsigned long long)(__double2ll_rz(v) + (1ll << 62));
-    c0[j] = (unsigned)u & 0x1FFFFFu;
-    c1[j] = (unsigned)(u >> 21) & 0x1FFFFFu;
-    c2[j] = (unsigned)(u >> 42);
+    lo[j] = (unsigned)u;
+    hi[j] = (unsigned)(u >> 32);
   }
   const int nk = min(8, K - (k0 + kg));
-  store_slices<0>(c0, c1, c2, *s_dev, out + (long long)r * kp + k0 + kg, plane, nk);
+  store_slices<0>(lo, hi, *s_dev, out + (long long)r * kp + k0 + kg, plane, nk);
 }
 
 // ---------------------------------------------------------- GEMM epilogue --
@@ -482,11 +513,10 @@ struct ResidueEpi {
   int accumulate;  // add onto the stored residue (K chunks after the first)
   __device__ __forceinline__ void operator()(int b, int p, int q0, const uint32_t (&v)[32]) const {
     if (p >= P || q0 >= Q) return;
-    // d mod m for |d| <= 2^30 (K <= 65536 products of |r| <= 128): e = d + bias
-    // lies in [0, 2^31 + 256), and floor(e * ceil(2^39/m) / 2^39) is exactly
-    // floor(e/m) because the excess e d' / 2^39 (d' < 1) stays below
-    // 1/256 + 2^-31 < 1/m for m <= 255 (and is 0 for m = 256).
-    const unsigned m = c_mod[b], bias = c_ebias[b], m39 = c_m39[b];
+    // d mod m for 0 <= d < 2^31 (K <= 32768 products of residues <= 255):
+    // floor(d * ceil(2^39/m) / 2^39) is exactly floor(d/m) because the excess
+    // d d' / 2^39 (d' < 1) stays below 2^-8 <= 1/m (and is 0 for m = 256).
+    const unsigned m = c_mod[b], m39 = c_m39[b];
     uint8_t *dst = R + (long long)b * plane + (long long)p * ldr + q0;
     uint32_t w[8];
 #pragma unroll
@@ -494,7 +524,7 @@ struct ResidueEpi {
       unsigned r4[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const unsigned e = v[4 * g + j] + bias;
+        const unsigned e = v[4 * g + j];
         r4[j] = e - (__umulhi(e, m39) >> 7) * m;
       }
       w[g] = __byte_perm(__byte_perm(r4[0], r4[1], 0x0040), __byte_perm(r4[2], r4[3], 0x0040),
@@ -530,158 +560,216 @@ __device__ __forceinline__ double byte_to_double(unsigned b) {  // exact, no con
   return __hiloint2double(0x43300000, (int)b) - 4503599627370496.0;
 }
 
-// C(m,n) = alpha * C'(m,n) 2^-(sigma_m + tau_n) + beta C(m,n).  C' is the value
-// in (-P/2, P/2) with the s residues: S = sum_i r_i W_i is accumulated exactly
-// in limbs held in doubles -- three 40-bit limbs when s <= 15 (r_i W_il <
-// 2^48, sums < 15 * 2^48 < 2^52), four 32-bit limbs for s = 16 -- the quotient
-// q = round(S/P) comes from one double estimate (|C'| <= P/4 keeps it exact),
-// S - qP is exact per limb (q P_l < 2^52), and the carries are settled in
-// 64-bit integers.  Each thread handles 4 consecutive rows m of one column n.
-// Rows/columns flagged NONFINITE use a direct FP64 dot product.
-template <int LIMBS>
-__global__ void __launch_bounds__(256)
-    reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr, int s,
-                       const int *__restrict__ s_dev, int M,
-                       int N, const int *__restrict__ sigA, const int *__restrict__ tauB,
-                       double alpha, double beta, double *__restrict__ C, int ldc,
+// The integer C' with residues r_i (value in (-P/2, P/2)) as a double, then
+// scaled: 2^-(sg + tg) C'.  S_l = sum_i r_i W_il are exact limb sums held in
+// doubles (three 40-bit limbs when S <= 15: r_i W_il < 2^48, sums < 15 * 2^48
+// < 2^52; four 32-bit limbs for S = 16); the quotient q = round(S/P) comes
+// from one double estimate (|C'| <= P/4 keeps it exact), S_l - q P_l is exact
+// per limb (q P_l < 2^52), and the carries are settled in 64-bit integers, so
+// C' is rounded once (exact whenever it is representable).
+template <int S>
+__device__ __forceinline__ double crt_value(const double (&Sl)[S <= 15 ? 3 : 4], int sg, int tg) {
+  constexpr int LIMBS = S <= 15 ? 3 : 4;
+  constexpr int LB = LIMBS == 3 ? 40 : 32;
+  double Sd = Sl[LIMBS - 1];
+#pragma unroll
+  for (int l = LIMBS - 2; l >= 0; --l) Sd = fma(Sd, (double)(1ull << LB), Sl[l]);
+  const double q = rint(Sd * c_invP[S]);
+  long long X[LIMBS];
+#pragma unroll
+  for (int l = 0; l < LIMBS; ++l) X[l] = __double2ll_rn(fma(-q, c_Pd[S][l], Sl[l]));
+#pragma unroll
+  for (int l = 0; l + 1 < LIMBS; ++l) {
+    const long long cy = X[l] >> LB;
+    X[l] -= cy * (1ll << LB);
+    X[l + 1] += cy;
+  }
+  unsigned long long lo;
+  long long hi;
+  if constexpr (LIMBS == 3) {  // X0 + X1 2^40 + X2 2^80, X0, X1 in [0, 2^40)
+    lo = (unsigned long long)X[0] | ((unsigned long long)X[1] << 40);
+    hi = (X[1] >> 24) + X[2] * 65536ll;
+  } else {  // X0 + X1 2^32 + X2 2^64 + X3 2^96, X0..X2 in [0, 2^32)
+    lo = ((unsigned long long)X[1] << 32) | (unsigned long long)X[0];
+    hi = X[3] * 4294967296ll + X[2];
+  }
+  // times 2^-(sg + tg) as two exact power-of-two factors: the first keeps the
+  // value normal, so the product rounds once (|C'| < 2^118: a remaining
+  // factor below 2^-1022 leaves less than the smallest subnormal, one above
+  // 2^1023 overflows any nonzero C')
+  const int ex = -(sg + tg);
+  const int e1 = ex > 1000 ? 1000 : (ex < -1000 ? -1000 : ex);
+  const int e2 = ex - e1;
+  const double f2 = e2 < -1022 ? 0.0 : pow2(e2 > 1023 ? 1023 : e2);
+  return (i128_to_double(hi, lo) * pow2(e1)) * f2;
+}
+
+// C(m,n) = alpha * C'(m,n) 2^-(sigma_m + tau_n) + beta C(m,n) for a modulus
+// count S fixed at compile time (so every CRT weight is an immediate operand
+// from the constant bank).  Each thread handles E consecutive rows m (8, or 4
+// with 16 moduli) and walks the columns n with the grid's y stride; per column
+// it issues every load first -- S residue words and the C pairs -- then
+// accumulates the limb sums (one byte-to-double conversion and LIMBS fused
+// multiply-adds per residue).  Rows/columns flagged NONFINITE use a direct
+// FP64 dot product.  Launched for the two possible counts of a call; the one
+// that is not the device-chosen count returns at once.
+template <int S>
+__global__ void __launch_bounds__(256, S <= 15 ? 2 : 1)
+    reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr,
+                       const int *__restrict__ s_dev, int M, int N,
+                       const int *__restrict__ sigA, const int *__restrict__ tauB, double alpha,
+                       double beta, double *__restrict__ C, int ldc,
                        const double *__restrict__ A, long long asr, long long ask,
                        const double *__restrict__ B, long long bsk, long long bsc, int K) {
-  static_assert(LIMBS == 3 || LIMBS == 4, "3 x 40-bit or 4 x 32-bit limbs");
-  constexpr int LB = LIMBS == 3 ? 40 : 32;
-  if (*s_dev != s) return;  // the launch for the other count does this call
-  // Grid: x covers the rows m in groups of 4 per thread, y strides over the
-  // columns n (no integer division per item).
-  const int m0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  constexpr int LIMBS = S <= 15 ? 3 : 4;
+  constexpr int E = LIMBS == 3 ? 8 : 4;  // rows per thread (the 4-limb form needs more registers)
+  constexpr int WPR = E / 4;             // 32-bit residue words per modulus
+  if (*s_dev != S) return;
+  const int m0 = (blockIdx.x * blockDim.x + threadIdx.x) * E;
   if (m0 >= M) return;
-  // C as two 16-byte pairs per thread when every 4-row group is 16-byte aligned
-  const bool vec = ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && ((ldc & 1) == 0);
-  const bool full = vec && m0 + 3 < M;
+  // residue words and C as vectors when every row group is aligned
+  const bool full = m0 + E <= M;
+  const bool rvec = full && ((reinterpret_cast<uintptr_t>(R) & (4 * WPR - 1)) == 0) &&
+                    ((ldr & (4 * WPR - 1)) == 0) && ((plane & (4 * WPR - 1)) == 0);
+  const bool cvec = full && ((reinterpret_cast<uintptr_t>(C) & 15) == 0) && ((ldc & 1) == 0);
+  int sg[E];
+  bool anydead = false;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    sg[e] = m0 + e < M ? sigA[m0 + e] : 0;
+    anydead |= sg[e] == NONFINITE;
+  }
   for (int n = blockIdx.y; n < N; n += gridDim.y) {
-    // Issue every load of this item first (s residue words, 4 C values): the
-    // pass is bound by memory latency unless they are all in flight together.
     const uint8_t *rp = R + (long long)n * ldr + m0;
-    unsigned w[OZ_MAX];
+    unsigned w[S][WPR];
 #pragma unroll
-    for (int i = 0; i < OZ_MAX; ++i)
-      w[i] = i < s ? __ldg(reinterpret_cast<const unsigned *>(rp + (long long)i * plane)) : 0u;
-    double *cp = C + (long long)n * ldc + m0;
-    double cold[4];
-    if (full) {
-      const double2 c01 = *reinterpret_cast<const double2 *>(cp);
-      const double2 c23 = *reinterpret_cast<const double2 *>(cp + 2);
-      cold[0] = c01.x; cold[1] = c01.y; cold[2] = c23.x; cold[3] = c23.y;
-    } else {
+    for (int i = 0; i < S; ++i) {
+      if (rvec) {
+        if constexpr (WPR == 2) {
+          const uint2 v = __ldg(reinterpret_cast<const uint2 *>(rp + (long long)i * plane));
+          w[i][0] = v.x;
+          w[i][WPR - 1] = v.y;
+        } else {
+          w[i][0] = __ldg(reinterpret_cast<const unsigned *>(rp + (long long)i * plane));
+        }
+      } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e) cold[e] = m0 + e < M ? cp[e] : 0.0;
-    }
-    double S[4][LIMBS];
+        for (int h = 0; h < WPR; ++h) {
+          unsigned x = 0;
 #pragma unroll
-    for (int e = 0; e < 4; ++e)
-#pragma unroll
-      for (int l = 0; l < LIMBS; ++l) S[e][l] = 0.0;
-#pragma unroll
-    for (int i = 0; i < OZ_MAX; ++i) {
-      if (i < s) {
-        double W[LIMBS];
-#pragma unroll
-        for (int l = 0; l < LIMBS; ++l) W[l] = c_Wd[s][i][l];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const double rd = byte_to_double((w[i] >> (8 * e)) & 0xFFu);
-#pragma unroll
-          for (int l = 0; l < LIMBS; ++l) S[e][l] = fma(rd, W[l], S[e][l]);
+          for (int e = 0; e < 4; ++e)
+            if (m0 + 4 * h + e < M) x |= (unsigned)rp[(long long)i * plane + 4 * h + e] << (8 * e);
+          w[i][h] = x;
         }
       }
     }
-    const int tg = tauB[n];
-    double out[4];
+    double *cp = C + (long long)n * ldc + m0;
+    double cold[E];
+    if (cvec) {
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int m = m0 + e;
-      out[e] = 0.0;
-      if (m >= M) continue;
-      const int sg = sigA[m];
-      double val;
-      if (sg == NONFINITE || tg == NONFINITE) {
+      for (int h = 0; h < E / 2; ++h) {
+        const double2 v = *reinterpret_cast<const double2 *>(cp + 2 * h);
+        cold[2 * h] = v.x;
+        cold[2 * h + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) cold[e] = m0 + e < M ? cp[e] : 0.0;
+    }
+    const int tg = tauB[n];
+    double Sl[E][LIMBS];
+#pragma unroll
+    for (int e = 0; e < E; ++e)
+#pragma unroll
+      for (int l = 0; l < LIMBS; ++l) Sl[e][l] = 0.0;
+#pragma unroll
+    for (int i = 0; i < S; ++i) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const double rd =
+            byte_to_double(__byte_perm(w[i][e >> 2], 0u, 0x4440u | (unsigned)(e & 3)));
+#pragma unroll
+        for (int l = 0; l < LIMBS; ++l) Sl[e][l] = fma(rd, c_Wd[S][i][l], Sl[e][l]);
+      }
+    }
+    double out[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      double val = crt_value<S>(Sl[e], sg[e], tg);
+      if ((anydead || tg == NONFINITE) && m0 + e < M && (sg[e] == NONFINITE || tg == NONFINITE)) {
         double acc = 0.0;
+        const int m = m0 + e;
         for (int k = 0; k < K; ++k) acc = fma(A[m * asr + k * ask], B[k * bsk + n * bsc], acc);
         val = acc;
-      } else {
-        double Sd = S[e][LIMBS - 1];
-#pragma unroll
-        for (int l = LIMBS - 2; l >= 0; --l) Sd = fma(Sd, (double)(1ull << LB), S[e][l]);
-        const double q = rint(Sd * c_invP[s]);
-        long long X[LIMBS];
-#pragma unroll
-        for (int l = 0; l < LIMBS; ++l) X[l] = __double2ll_rn(fma(-q, c_Pd[s][l], S[e][l]));
-#pragma unroll
-        for (int l = 0; l + 1 < LIMBS; ++l) {
-          const long long cy = X[l] >> LB;
-          X[l] -= cy * (1ll << LB);
-          X[l + 1] += cy;
-        }
-        unsigned long long lo;
-        long long hi;
-        if constexpr (LIMBS == 3) {  // X0 + X1 2^40 + X2 2^80, X0, X1 in [0, 2^40)
-          lo = (unsigned long long)X[0] | ((unsigned long long)X[1] << 40);
-          hi = (X[1] >> 24) + X[2] * 65536ll;
-        } else {  // X0 + X1 2^32 + X2 2^64 + X3 2^96, X0..X2 in [0, 2^32)
-          lo = ((unsigned long long)X[1] << 32) | (unsigned long long)X[0];
-          hi = X[3] * 4294967296ll + X[2];
-        }
-        // times 2^-(sg + tg) as two exact power-of-two factors: the first
-        // keeps the value normal, so the product rounds once
-        // (|C'| < 2^118: a remaining factor below 2^-1022 leaves less than the
-        // smallest subnormal, one above 2^1023 overflows any nonzero C')
-        const int ex = -(sg + tg);
-        const int e1 = ex > 1000 ? 1000 : (ex < -1000 ? -1000 : ex);
-        const int e2 = ex - e1;
-        const double f2 = e2 < -1022 ? 0.0 : pow2(e2 > 1023 ? 1023 : e2);
-        val = (i128_to_double(hi, lo) * pow2(e1)) * f2;
       }
       out[e] = (beta == 1.0) ? fma(alpha, val, cold[e]) : fma(alpha, val, beta * cold[e]);
     }
-    if (full) {
-      *reinterpret_cast<double2 *>(cp) = make_double2(out[0], out[1]);
-      *reinterpret_cast<double2 *>(cp + 2) = make_double2(out[2], out[3]);
+    if (cvec) {
+#pragma unroll
+      for (int h = 0; h < E / 2; ++h)
+        *reinterpret_cast<double2 *>(cp + 2 * h) = make_double2(out[2 * h], out[2 * h + 1]);
     } else {
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
+      for (int e = 0; e < E; ++e)
         if (m0 + e < M) cp[e] = out[e];
     }
   }
 }
 
-// Launch of the reconstruction with the limb width the modulus count allows.
+// Grid: x covers the row groups (8 rows per thread, 4 with 16 moduli; 256
+// threads per block); y strides over the columns.  ymax caps the y extent.
+template <int S>
+void launch_reconstruct_s(unsigned ymax, cudaStream_t st, const uint8_t *R, long long plane,
+                          int ldr, const int *s_dev, int M, int N, const int *sigA,
+                          const int *tauB, double alpha, double beta, double *C, int ldc,
+                          const double *A, long long asr, long long ask, const double *B,
+                          long long bsk, long long bsc, int K) {
+  constexpr int E = S <= 15 ? 8 : 4;
+  const unsigned bx = (unsigned)(((M + E - 1) / E + 255) / 256);
+  unsigned by = (unsigned)N < ymax ? (unsigned)N : ymax;
+  if (by < 1u) by = 1u;
+  reconstruct_kernel<S><<<dim3(bx, by), 256, 0, st>>>(R, plane, ldr, s_dev, M, N, sigA, tauB,
+                                                      alpha, beta, C, ldc, A, asr, ask, B, bsk,
+                                                      bsc, K);
+}
+
+template <int S>
+void launch_reconstruct_any(int s, unsigned ymax, cudaStream_t st, const uint8_t *R,
+                            long long plane, int ldr, const int *s_dev, int M, int N,
+                            const int *sigA, const int *tauB, double alpha, double beta,
+                            double *C, int ldc, const double *A, long long asr, long long ask,
+                            const double *B, long long bsk, long long bsc, int K) {
+  if constexpr (S <= OZ_MAX) {
+    if (s == S)
+      launch_reconstruct_s<S>(ymax, st, R, plane, ldr, s_dev, M, N, sigA, tauB, alpha, beta, C,
+                              ldc, A, asr, ask, B, bsk, bsc, K);
+    else
+      launch_reconstruct_any<S + 1>(s, ymax, st, R, plane, ldr, s_dev, M, N, sigA, tauB, alpha,
+                                    beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
+  }
+}
+
+// Launch of the reconstruction for the call's possible modulus counts; each
+// launch returns at once unless the device-chosen count is its own.
 void launch_reconstruct(const uint8_t *R, long long plane, int ldr, const int *s_dev, int s_lo,
                         int s_hi, int M, int N,
                         const int *sigA, const int *tauB, double alpha, double beta, double *C,
                         int ldc, const double *A, long long asr, long long ask, const double *B,
                         long long bsk, long long bsc, int K, cudaStream_t st) {
-  const dim3 blocks((unsigned)(((M + 3) / 4 + 255) / 256), (unsigned)(N < 65535 ? N : 65535));
-  // one launch per possible count (s_lo, and s_hi when it differs); each
-  // returns at once unless the device-chosen count is its own
-  if (s_lo <= 15)
-    reconstruct_kernel<3><<<blocks, 256, 0, st>>>(R, plane, ldr, s_lo, s_dev, M, N, sigA, tauB,
-                                                   alpha, beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
-  else
-    reconstruct_kernel<4><<<blocks, 256, 0, st>>>(R, plane, ldr, s_lo, s_dev, M, N, sigA, tauB,
-                                                   alpha, beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
+  // each thread walks about four columns, so its set-up (row exponents) is
+  // amortised
+  const unsigned ymax = (unsigned)((N + 3) / 4 < 65535 ? (N + 3) / 4 : 65535);
+  launch_reconstruct_any<2>(s_lo, ymax, st, R, plane, ldr, s_dev, M, N, sigA, tauB, alpha, beta, C,
+                            ldc, A, asr, ask, B, bsk, bsc, K);
   if (s_hi != s_lo) {
     // The heavy-tail count is the rare one: this launch usually exits at
     // once, and a grid of about 8 blocks per SM (columns strided) keeps that
     // cheap.
-    dim3 b4 = blocks;
-    {
-      const unsigned y = 1184u / (blocks.x > 0 ? blocks.x : 1u);
-      b4.y = y < 1u ? 1u : (y < blocks.y ? y : blocks.y);
-    }
-    if (s_hi <= 15)
-      reconstruct_kernel<3><<<b4, 256, 0, st>>>(R, plane, ldr, s_hi, s_dev, M, N, sigA, tauB, alpha,
-                                                beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
-    else
-      reconstruct_kernel<4><<<b4, 256, 0, st>>>(R, plane, ldr, s_hi, s_dev, M, N, sigA, tauB, alpha,
-                                                beta, C, ldc, A, asr, ask, B, bsk, bsc, K);
+    const unsigned bx = (unsigned)(((M + 3) / 4 + 255) / 256);
+    unsigned y = 1184u / (bx > 0 ? bx : 1u);
+    y = y < 1u ? 1u : (y < ymax ? y : ymax);
+    launch_reconstruct_any<2>(s_hi, y, st, R, plane, ldr, s_dev, M, N, sigA, tauB, alpha, beta, C,
+                              ldc, A, asr, ask, B, bsk, bsc, K);
   }
 }
 
@@ -700,11 +788,10 @@ int upload_tables(int dev, cudaStream_t st) {
   if (dev < 0 || dev >= 64) return B2_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lk(g_table_mu);
   if (g_table_done[dev]) return B2_OK;
-  unsigned mod[OZ_MAX], ebias[OZ_MAX], m39[OZ_MAX];
+  unsigned mod[OZ_MAX], m39[OZ_MAX];
   for (int i = 0; i < OZ_MAX; ++i) {
     const unsigned long long m = (unsigned long long)kModuli[i];
     mod[i] = (unsigned)m;
-    ebias[i] = (unsigned)(m * (((1ull << 30) + m - 1) / m));
     m39[i] = (unsigned)(((1ull << 39) + m - 1) / m);
   }
   static double wd[OZ_MAX + 1][OZ_MAX][4], pd[OZ_MAX + 1][4], ip[OZ_MAX + 1];
@@ -718,7 +805,6 @@ int upload_tables(int dev, cudaStream_t st) {
     ip[s] = t.invP;
   }
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_mod, mod, sizeof(mod), 0, cudaMemcpyHostToDevice, st));
-  B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_ebias, ebias, sizeof(ebias), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_m39, m39, sizeof(m39), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Wd, wd, sizeof(wd), 0, cudaMemcpyHostToDevice, st));
   B2_CUDA_TRY(cudaMemcpyToSymbolAsync(c_Pd, pd, sizeof(pd), 0, cudaMemcpyHostToDevice, st));
@@ -791,29 +877,29 @@ struct ASideCache {
 };
 thread_local ASideCache g_aside;
 
-int run_i8_gemm(int variant, const int8_t *X, const int8_t *Y, long long kcl, int n, int m, int s,
+int run_i8_gemm(int variant, const uint8_t *X, const uint8_t *Y, long long kcl, int n, int m, int s,
                 long long kp, long long planeX, long long planeY, const ResidueEpi &epi,
                 int device, int sm_count, int *derr, cudaStream_t st, const int *s_dev) {
   const int ybox = variant == 0 ? 256 : 128;  // pair variants stage BN/2 = 128 rows per CTA
   CUtensorMap tmX, tmY;
-  int rc = umma::make_kmajor_map(&tmX, umma::KIND_I8, X, kcl, n, s, kp, planeX, umma::BM);
-  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, kcl, m, s, kp, planeY, ybox);
+  int rc = umma::make_kmajor_map(&tmX, umma::KIND_U8, X, kcl, n, s, kp, planeX, umma::BM);
+  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_U8, Y, kcl, m, s, kp, planeY, ybox);
   if (rc != B2_OK) return rc;
   switch (variant) {
     case 1:
-      return umma::launch<umma::KIND_I8, 128, 6>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
+      return umma::launch<umma::KIND_U8, 128, 6>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
                                                   "ozaki_i8_gemm", 0, s_dev);
     case 2:
-      return umma::launch<umma::KIND_I8, 128, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
+      return umma::launch<umma::KIND_U8, 128, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
                                                   "ozaki_i8_gemm", 0, s_dev);
     case 3:
-      return umma::launch_pair<umma::KIND_I8, 256, 6>(tmX, tmY, n, m, kcl, s, epi, device, derr,
+      return umma::launch_pair<umma::KIND_U8, 256, 6>(tmX, tmY, n, m, kcl, s, epi, device, derr,
                                                        st, "ozaki_i8_gemm", s_dev);
     case 4:
-      return umma::launch_pair<umma::KIND_I8, 256, 7>(tmX, tmY, n, m, kcl, s, epi, device, derr,
+      return umma::launch_pair<umma::KIND_U8, 256, 7>(tmX, tmY, n, m, kcl, s, epi, device, derr,
                                                        st, "ozaki_i8_gemm", s_dev);
     default:
-      return umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
+      return umma::launch<umma::KIND_U8, 256, 4>(tmX, tmY, n, m, kcl, s, epi, sm_count, derr, st,
                                                   "ozaki_i8_gemm", 0, s_dev);
   }
 }
@@ -868,8 +954,8 @@ int norm_exponents(const double *X, long long sr, long long sk, int R, int K, in
   B2_CUDA_TRY(cudaGetLastError());
   {
     B2_PROF("ozaki_norm_finalize", s);
-    norm_finalize_kernel<<<(R + 255) / 256, 256, 0, s>>>(pmax, pssq, pl1, R, chunks, H, sigma, X,
-                                                          sr, sk, K, stat);
+    norm_finalize_kernel<<<(R + 31) / 32, 32 * FIN_WARPS, 0, s>>>(pmax, pssq, pl1, R, chunks, H,
+                                                                   sigma, X, sr, sk, K, stat);
   }
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
@@ -944,7 +1030,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   // op(B) columns as n x K rows: element (j,k) at B[j*bsr + k*bsk]
   const long long bsr = tB ? 1 : ldb, bsk = tB ? ldb : 1;
 
-  const int KCH = 1 << 16;  // K per INT32-exact GEMM pass (|sum| < 2^30)
+  const int KCH = OZ_KCHUNK;  // K per INT32-exact GEMM pass
   const int kchunks = (k + KCH - 1) / KCH;
   const long long kp = round_up(k < KCH ? k : KCH, 16);
   const long long mp = round_up(m, 16);
@@ -959,8 +1045,8 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   const long long planeY = (long long)m_all * kp, planeX = (long long)n * kp;
   const long long planeR = (long long)n * mp;
 
-  int8_t *Yall = (int8_t *)workspace(cx, WS_OZ_Y, (size_t)planeY * s_max);
-  int8_t *X = (int8_t *)workspace(cx, WS_OZ_X, (size_t)planeX * s_max);
+  uint8_t *Yall = (uint8_t *)workspace(cx, WS_OZ_Y, (size_t)planeY * s_max);
+  uint8_t *X = (uint8_t *)workspace(cx, WS_OZ_X, (size_t)planeX * s_max);
   uint8_t *Rb = (uint8_t *)workspace(cx, WS_OZ_R, (size_t)planeR * s_max);
   const size_t nsA = norm_scratch_bytes(m, k), nsB = norm_scratch_bytes(n, k);
   // [sigma (m_all)|tau][stat A (2 doubles), stat B (2 doubles), modulus count][norm A][norm B]
@@ -971,7 +1057,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   if (!Yall || !X || !Rb || !sc) return B2_ERR_NOMEM;
   int *sigA = (int *)sc + r0;
   int *tauB = (int *)sc + m_all;
-  int8_t *Y = Yall + (long long)r0 * kp;
+  uint8_t *Y = Yall + (long long)r0 * kp;
   double *stat = (double *)(sc + o_stat);
   int *s_dev = (int *)(stat + 4);
   void *scrA = sc + o_scr;
@@ -1004,7 +1090,80 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
     B2_CUDA_TRY(cudaGetLastError());
   }
 
-  for (int c = 0; c < kchunks && rc == B2_OK; ++c) {
+  // Overlapped schedule for large single-pass products: B and C in J column
+  // blocks; the INT8 GEMM of block j (tensor-bound, little HBM traffic) runs
+  // on a high-priority stream while the slicing of later blocks and the
+  // reconstruction of earlier ones (HBM- and FP64-bound) run beside it on an
+  // auxiliary stream, so most of the auxiliary passes hide under the GEMMs.
+  const int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
+                 (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
+                    ? (n / 2048 < 2 ? 2 : (n / 2048 > 8 ? 8 : n / 2048))
+                    : 1;
+  if (J > 1) {
+    const int nb = (int)round_up((n + J - 1) / J, 256);
+    const int nblk = (n + nb - 1) / nb;
+    cudaStream_t gs = cx->oz_gemm, as = cx->oz_aux;
+    // events: [0, 16) block sliced, [16, 32) block multiplied, 32 fork, 33/34 joins
+    cudaEvent_t *ev = cx->oz_ev;
+    auto slice_b = [&](int j, cudaStream_t s2) {
+      const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
+      dim3 grid((k + 63) / 64, (nj + 31) / 32);
+      B2_PROF(bsr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", s2);
+      if (bsr == 1)
+        slice_kernel<true><<<grid, 256, 0, s2>>>(B + j0 * bsr, bsr, bsk, nj, k, tauB + j0, s_dev,
+                                                 X + (long long)j0 * kp, kp, planeX);
+      else
+        slice_kernel<false><<<grid, 256, 0, s2>>>(B + j0 * bsr, bsr, bsk, nj, k, tauB + j0, s_dev,
+                                                  X + (long long)j0 * kp, kp, planeX);
+    };
+    {
+      dim3 grid((k + 63) / 64, (m + 31) / 32);
+      B2_PROF(asr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
+      if (asr == 1)
+        slice_kernel<true><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s_dev, Y, kp, planeY);
+      else
+        slice_kernel<false><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s_dev, Y, kp, planeY);
+      B2_CUDA_TRY(cudaGetLastError());
+    }
+    slice_b(0, st);
+    B2_CUDA_TRY(cudaGetLastError());
+    B2_CUDA_TRY(cudaEventRecord(ev[32], st));  // exponents, count, A and block 0 sliced
+    B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[32], 0));
+    B2_CUDA_TRY(cudaStreamWaitEvent(as, ev[32], 0));
+    for (int j = 1; j < nblk; ++j) {
+      slice_b(j, as);
+      B2_CUDA_TRY(cudaGetLastError());
+      B2_CUDA_TRY(cudaEventRecord(ev[j], as));
+    }
+    for (int j = 0; j < nblk && rc == B2_OK; ++j) {
+      const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
+      if (j > 0) B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[j], 0));
+      ResidueEpi epi{Rb + (long long)j0 * mp, planeR, (int)mp, nj, m, 0};
+      rc = run_i8_gemm(g_oz_variant, X + (long long)j0 * kp, Y, k, nj, m, s_max, kp, planeX,
+                       planeY, epi, cx->device, cx->sm_count, cx->derr, gs, s_dev);
+      if (rc == B2_OK) rc = cudaEventRecord(ev[16 + j], gs) == cudaSuccess ? B2_OK : B2_ERR_CUDA;
+    }
+    for (int j = 0; j < nblk && rc == B2_OK; ++j) {
+      const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
+      B2_CUDA_TRY(cudaStreamWaitEvent(as, ev[16 + j], 0));
+      B2_PROF("ozaki_reconstruct", as);
+      launch_reconstruct(Rb + (long long)j0 * mp, planeR, (int)mp, s_dev, s_base, s_max, m, nj,
+                         sigA, tauB + j0, alpha, beta, C + (long long)j0 * ldc, ldc, A, asr, ask,
+                         B + j0 * bsr, bsk, bsr, k, as);
+      B2_CUDA_TRY(cudaGetLastError());
+    }
+    // join: the caller's stream waits for both streams (also on an error, so
+    // nothing of this call is left running unordered)
+    cudaError_t e1 = cudaEventRecord(ev[33], as);
+    if (e1 == cudaSuccess) e1 = cudaStreamWaitEvent(st, ev[33], 0);
+    cudaError_t e2 = cudaEventRecord(ev[34], gs);
+    if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(st, ev[34], 0);
+    if (rc != B2_OK) return rc;
+    if (e1 != cudaSuccess) return cuda_fail(e1, "ozaki overlap join");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "ozaki overlap join");
+  }
+
+  for (int c = 0; c < kchunks && rc == B2_OK && J == 1; ++c) {
     const int kc0 = c * KCH, kcl = (k - kc0 < KCH) ? k - kc0 : KCH;
     if (!reuse_a) {
       dim3 grid((kcl + 63) / 64, (m + 31) / 32);
@@ -1033,7 +1192,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
                      cx->sm_count, cx->derr, st, s_dev);
   }
   if (rc != B2_OK) return rc;
-  {
+  if (J == 1) {
     B2_PROF("ozaki_reconstruct", st);
     launch_reconstruct(Rb, planeR, (int)mp, s_dev, s_base, s_max, m, n, sigA, tauB, alpha, beta, C,
                        ldc, A, asr, ask, B, bsk, bsr, k, st);
@@ -1083,7 +1242,7 @@ extern "C" int b2_ozaki_last_plan(int *out, int n) {
 //   [error word][modulus count][sigma|tau][norm scratch A|B][Y][X][R]
 // The call needs s*(m*kp + n*kp + n*mp) + (m + n)*4 + the norm scratch
 // (24 bytes per row and K chunk) + alignment, kp = K rounded up to 16
-// (K <= 65536), mp = m rounded up to 16; a larger problem is refused with
+// (K <= 32768), mp = m rounded up to 16; a larger problem is refused with
 // B2_ERR_ARG before anything is launched.  Device pointers only (checked by
 // the caller).  Nothing here allocates.
 // ---------------------------------------------------------------------------
@@ -1107,7 +1266,7 @@ int ozaki_noalloc_run(unsigned char *base, size_t cap, int dev, int sm_count, ch
                       cudaStream_t st) {
   const int s = slices > 0 ? slices : ozaki_auto_moduli(k);
   if (s < 2 || s > OZ_MAX) return B2_ERR_ARG;
-  if (k > (1 << 16)) return B2_ERR_ARG;  // one exact INT32 pass only
+  if (k > OZ_KCHUNK) return B2_ERR_ARG;  // one exact INT32 pass only
   if (ozaki_noalloc_bytes(m, n, k, s) > cap) return B2_ERR_ARG;
 
   const long long kp = round_up(k, 16), mp = round_up(m, 16);
@@ -1131,8 +1290,8 @@ int ozaki_noalloc_run(unsigned char *base, size_t cap, int dev, int sm_count, ch
   int *s_dev = (int *)(base + 64);  // modulus count read by the kernels (set below)
   int *sigA = (int *)(base + o_sig);
   int *tauB = sigA + m;
-  int8_t *Y = (int8_t *)(base + o_Y);
-  int8_t *X = (int8_t *)(base + o_X);
+  uint8_t *Y = (uint8_t *)(base + o_Y);
+  uint8_t *X = (uint8_t *)(base + o_X);
   uint8_t *Rb = (uint8_t *)(base + o_R);
   // the error word is the only state that must start at zero
   B2_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), st));
@@ -1169,11 +1328,11 @@ int ozaki_noalloc_run(unsigned char *base, size_t cap, int dev, int sm_count, ch
     B2_CUDA_TRY(cudaGetLastError());
   }
   CUtensorMap tmX, tmY;
-  rc = umma::make_kmajor_map(&tmX, umma::KIND_I8, X, k, n, s, kp, planeX, umma::BM);
-  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_I8, Y, k, m, s, kp, planeY, 256);
+  rc = umma::make_kmajor_map(&tmX, umma::KIND_U8, X, k, n, s, kp, planeX, umma::BM);
+  if (rc == B2_OK) rc = umma::make_kmajor_map(&tmY, umma::KIND_U8, Y, k, m, s, kp, planeY, 256);
   if (rc != B2_OK) return rc;
   ResidueEpi epi{Rb, planeR, (int)mp, n, m, 0};
-  rc = umma::launch<umma::KIND_I8, 256, 4>(tmX, tmY, n, m, k, s, epi, sm_count, derr, st,
+  rc = umma::launch<umma::KIND_U8, 256, 4>(tmX, tmY, n, m, k, s, epi, sm_count, derr, st,
                                             "ozaki_i8_gemm");
   if (rc != B2_OK) return rc;
   launch_reconstruct(Rb, planeR, (int)mp, s_dev, s, s, m, n, sigA, tauB, alpha, beta, C, ldc, A,

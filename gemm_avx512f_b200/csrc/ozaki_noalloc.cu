@@ -88,7 +88,7 @@ extern "C" int b2_dgemm_ozaki_noalloc(char transa, char transb, int m, int n, in
   const int s = slices > 0 ? slices : ozaki_auto_moduli(k);
   const bool product = k > 0 && alpha != 0.0;
   // size limit first, so an oversized call is refused before any set-up
-  if (product && (k > (1 << 16) || ozaki_noalloc_bytes(m, n, k, s) > B2_NOALLOC_SCRATCH_BYTES))
+  if (product && (k > (1 << 15) || ozaki_noalloc_bytes(m, n, k, s) > B2_NOALLOC_SCRATCH_BYTES))
     return B2_ERR_ARG;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {

@@ -34,7 +34,7 @@ int make_kmajor_map(CUtensorMap *map, int kind, const void *base, long long kele
   if (((uintptr_t)base & 15) || (row_bytes & 15) || (plane_bytes & 15) || box_rows < 1 ||
       box_rows > 256)
     return B2_ERR_ARG;
-  const CUtensorMapDataType dt = kind == KIND_I8     ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+  const CUtensorMapDataType dt = is_int8(kind)      ? CU_TENSOR_MAP_DATA_TYPE_UINT8
                                  : kind == KIND_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
                                                      : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   cuuint64_t dims[3] = {(cuuint64_t)kelems, (cuuint64_t)rows, (cuuint64_t)nbatch};

@@ -39,7 +39,9 @@
 namespace b2 {
 namespace umma {
 
-enum Kind { KIND_I8 = 0, KIND_BF16 = 1, KIND_TF32 = 2 };
+// KIND_I8: signed 8-bit operands, KIND_U8: unsigned 8-bit (both kind::i8, S32
+// accumulators); KIND_BF16: kind::f16 with BF16 operands; KIND_TF32: kind::tf32.
+enum Kind { KIND_I8 = 0, KIND_BF16 = 1, KIND_TF32 = 2, KIND_U8 = 3 };
 
 constexpr int BM = 128;            // accumulator lanes (X rows) per tile
 constexpr int KBLOCK_BYTES = 128;  // one 128B swizzle atom along K per stage
@@ -60,15 +62,17 @@ inline void launch_wait_settings(uint64_t *wait_ns, int *withhold) {
   *withhold = w > 0 ? 1 : 0;
 }
 
-__host__ __device__ constexpr int elem_bytes(int kind) { return kind == KIND_I8 ? 1 : kind == KIND_BF16 ? 2 : 4; }
+__host__ __device__ constexpr bool is_int8(int kind) { return kind == KIND_I8 || kind == KIND_U8; }
+__host__ __device__ constexpr int elem_bytes(int kind) { return is_int8(kind) ? 1 : kind == KIND_BF16 ? 2 : 4; }
 
 // Instruction descriptor (PTX ISA tcgen05 "instruction descriptor" for
 // .kind::f16 / .kind::tf32 / .kind::i8): D format at [4,6), A/B formats at
 // [7,10)/[10,13), K-major A and B (bits 15/16 clear), N>>3 at [17,23),
 // M>>4 at [24,29).
 __host__ __device__ constexpr uint32_t make_idesc(int kind, int m, int n) {
-  const uint32_t dfmt = kind == KIND_I8 ? 2u : 1u;       // S32 : F32
-  const uint32_t abfmt = kind == KIND_I8 ? 1u             // signed 8-bit
+  const uint32_t dfmt = is_int8(kind) ? 2u : 1u;        // S32 : F32
+  const uint32_t abfmt = kind == KIND_U8 ? 0u             // unsigned 8-bit
+                         : kind == KIND_I8 ? 1u           // signed 8-bit
                          : kind == KIND_BF16 ? 1u          // BF16
                                              : 2u;         // TF32
   return (dfmt << 4) | (abfmt << 7) | (abfmt << 10) | ((uint32_t)(n >> 3) << 17) |
@@ -170,7 +174,7 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
 template <int KIND>
 __device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                        uint32_t idesc, uint32_t accumulate) {
-  if constexpr (KIND == KIND_I8) {
+  if constexpr (is_int8(KIND)) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
@@ -532,7 +536,7 @@ __device__ __forceinline__ void tc_commit_pair(uint32_t bar, uint16_t mask) {
 template <int KIND>
 __device__ __forceinline__ void tc_mma_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                             uint32_t idesc, uint32_t accumulate) {
-  if constexpr (KIND == KIND_I8) {
+  if constexpr (is_int8(KIND)) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),

@@ -163,7 +163,7 @@ B2_API int b2_dgemm_multi(int ndev, const int *devices, char transa, char transb
                           int ldb, double beta, double *C, int ldc, int method, int slices);
 
 /* Plan of the last Ozaki DGEMM on this thread: out[0] = modulus (slice)
- * count, out[1] = number of K chunks (K is cut at 65536 per exact INT32 pass).
+ * count, out[1] = number of K chunks (K is cut at 32768 per exact INT32 pass).
  * With slices = 0 the count (15, or 16 for heavy-tailed rows) is chosen on the
  * device; this call waits for that choice to be copied back. */
 B2_API int b2_ozaki_last_plan(int *out, int n);
@@ -181,7 +181,7 @@ B2_API int b2_ozaki_last_plan(int *out, int n);
  * CUDA default) it is reserved on a device at the first call there and held
  * until the process exits; processes that never call this entry point do not
  * pay for it.  Limit: problems whose scratch exceeds the array -- square ones
- * above n = 1200 at 15 moduli (1161 at 16), or K > 65536 -- return
+ * above n = 1200 at 15 moduli (1161 at 16), or K > 32768 -- return
  * B2_ERR_ARG without touching C.  Every call on a device shares the array and
  * it keeps the last call's contents, so calls that overlap on the GPU race
  * and must be serialised by the caller.  The first call on a device resolves

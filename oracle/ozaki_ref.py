@@ -7,7 +7,7 @@ scaling rule and the same residue conventions as the library, so the GPU
 pipeline can be checked stage by stage on small inputs:
 
     sigma_i = H - ceil(log2 ||a_i||_2),  A'_ik = trunc(a_ik 2^sigma_i)
-    r_t     = symmetric residue of A' (resp. B') mod m_t      (int8)
+    r_t     = A' (resp. B') mod m_t in [0, m_t)             (uint8)
     D_t     = r_t(A) r_t(B) mod m_t                           (exact)
     C'      = CRT(D_1 .. D_s) in (-P/2, P/2)
     C       = alpha * C' 2^-(sigma_i + tau_j) + beta * C
@@ -49,11 +49,9 @@ def row_sigma(x: np.ndarray, H: int) -> np.ndarray:
     return out
 
 
-def sym_residue(x: int, m: int) -> int:
-    r = x % m
-    if r > (m - 1) // 2:
-        r -= m
-    return r
+def residue(x: int, m: int) -> int:
+    """x mod m in [0, m) (Python's % is non-negative for m > 0)."""
+    return x % m
 
 
 def emulate(transa, transb, m, n, k, alpha, a, b, beta, c, s=14):
@@ -79,7 +77,7 @@ def emulate(transa, transb, m, n, k, alpha, a, b, beta, c, s=14):
             else:
                 acc = 0
                 for t, mt in enumerate(mods):
-                    d = sum(sym_residue(ia[i][kk], mt) * sym_residue(ib[j][kk], mt)
+                    d = sum(residue(ia[i][kk], mt) * residue(ib[j][kk], mt)
                             for kk in range(k)) % mt
                     acc += d * W[t]
                 x = acc % P

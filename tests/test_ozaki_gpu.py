@@ -140,7 +140,7 @@ def test_long_k_is_chunked(cuda):
     got = _run(cuda, "N", "N", m, n, k, 1.0, a, b, 0.0, c)
     plan = (__import__("ctypes").c_int * 2)()
     _lib.lib().b2_ozaki_last_plan(plan, 2)
-    assert plan[1] == 2
+    assert plan[1] == -(-k // 32768)  # exact INT32 passes of at most 32768
     assert normalized(got, ref, k, a, b, U) <= 8
 
 
