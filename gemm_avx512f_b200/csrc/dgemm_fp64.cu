@@ -15,8 +15,9 @@
 //    bank-conflict free for both orientations (+4 doubles per row).
 //  * alpha/beta are applied once in the epilogue (the reference folds alpha
 //    into packed B, src/gemm_copy.c:64, and pre-scales C, :131).
-//  * Optional split-K: each z-slice writes an FP64 partial into workspace and a
-//    reduction kernel applies alpha/beta deterministically.
+//  * Optional split-K: each z-slice writes an FP64 partial into workspace and
+//    the tile's last slice to finish adds them in slice order (deterministic)
+//    and applies alpha/beta -- no separate reduction launch.
 #include "b2_internal.cuh"
 #include "b2_profile.cuh"
 
@@ -102,14 +103,17 @@ __device__ __forceinline__ void dmma(double (&c)[4], const double *a, const doub
 
 // A_KCONT = transA (op(A)(m,k) = A[m*lda+k]); B_KCONT = !transB (op(B)(k,n) = B[n*ldb+k]).
 // Output: when P != nullptr the raw product of this CTA's K range is written to
-// P + z*ldp*N (split-K partial); otherwise C = alpha*acc + beta*C (beta==1: C += alpha*acc).
+// P + z*ldp*N (split-K partial) and the last of the tile's gridDim.z CTAs to
+// arrive (counted in cnt[tile], which it resets to zero for the next launch)
+// adds the partials in slice order, still in L2, and writes
+// C = alpha*sum + beta*C; otherwise C = alpha*acc + beta*C (beta==1: C += alpha*acc).
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MMAK, bool A_KCONT,
           bool B_KCONT, int VEC>
 __global__ void __launch_bounds__(WM *WN * 32, 1)
     dgemm_dmma_kernel(int M, int N, int K, int kchunk, double alpha,
                       const double *__restrict__ A, int lda, const double *__restrict__ B,
                       int ldb, double beta, double *__restrict__ C, int ldc,
-                      double *__restrict__ P, int ldp) {
+                      double *__restrict__ P, int ldp, int *__restrict__ cnt) {
   constexpr int NT = WM * WN * 32;
   constexpr int TM = BM / WM, TN = BN / WN;  // warp tile
   constexpr int MT = TM / 16, NTL = TN / 8;
@@ -202,6 +206,30 @@ __global__ void __launch_bounds__(WM *WN * 32, 1)
           const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
           if (m < M && n < N) Pz[(size_t)n * ldp + m] = acc[i][j][v];
         }
+    // In-kernel fixup: every slice publishes its partial (fence, then one
+    // arrival); the last to arrive sums all slices of the tile in order.
+    __shared__ int last_slice;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+      const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+      const int prev = atomicAdd(cnt + tile, 1);
+      last_slice = prev == (int)gridDim.z - 1;
+      if (last_slice) cnt[tile] = 0;  // every slice has arrived: ready for the next launch
+    }
+    __syncthreads();
+    if (!last_slice) return;
+    __threadfence();
+    const bool one = (beta == 1.0);
+    for (int idx = tid; idx < BM * BN; idx += NT) {
+      const int m = m0 + idx % BM, n = n0 + idx / BM;
+      if (m >= M || n >= N) continue;
+      const double *pp = P + (size_t)n * ldp + m;
+      double sum = 0.0;
+      for (int z = 0; z < (int)gridDim.z; ++z) sum += __ldcg(pp + (size_t)z * ldp * N);
+      double *c = C + (size_t)n * ldc + m;
+      *c = one ? fma(alpha, sum, *c) : fma(alpha, sum, beta * *c);
+    }
     return;
   }
   const bool beta_one = (beta == 1.0);
@@ -219,21 +247,6 @@ __global__ void __launch_bounds__(WM *WN * 32, 1)
           *p = beta_one ? fma(alpha, acc[i][j][v], c_old) : fma(alpha, acc[i][j][v], beta * c_old);
         }
       }
-}
-
-// C = alpha * sum_z P[z] + beta*C   (beta==1: C += ...)
-__global__ void splitk_reduce_kernel(int M, int N, int splits, const double *__restrict__ P,
-                                     int ldp, double alpha, double beta, double *__restrict__ C,
-                                     int ldc) {
-  const size_t total = (size_t)M * N;
-  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
-       idx += (size_t)gridDim.x * blockDim.x) {
-    const int m = (int)(idx % M), n = (int)(idx / M);
-    double s = 0.0;
-    for (int z = 0; z < splits; ++z) s += P[(size_t)z * ldp * N + (size_t)n * ldp + m];
-    double *p = C + (size_t)n * ldc + m;
-    *p = (beta == 1.0) ? fma(alpha, s, *p) : fma(alpha, s, beta * *p);
-  }
 }
 
 template <typename T>
@@ -259,6 +272,7 @@ struct LaunchArgs {
   double *P;
   int ldp;
   int splits;
+  int *cnt;  // per-tile arrival counters of the split-K fixup (zero between launches)
 };
 
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MMAK, bool AK, bool BKc,
@@ -274,7 +288,7 @@ cudaError_t launch_one(const LaunchArgs &a, cudaStream_t s) {
   dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, a.splits);
   B2_PROF("dgemm_dmma", s);
   kern<<<grid, WM * WN * 32, SMEM, s>>>(a.M, a.N, a.K, a.kchunk, a.alpha, a.A, a.lda, a.B, a.ldb,
-                                        a.beta, a.C, a.ldc, a.P, a.ldp);
+                                        a.beta, a.C, a.ldc, a.P, a.ldp, a.cnt);
   return cudaGetLastError();
 }
 
@@ -360,7 +374,7 @@ int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double
   const bool bk = is_notrans(tb);   // plain B: k contiguous
   const bool vec2 = (lda % 2 == 0) && (ldb % 2 == 0) && (((uintptr_t)A & 15) == 0) &&
                     (((uintptr_t)B & 15) == 0);
-  LaunchArgs a{m, n, k, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0, 1};
+  LaunchArgs a{m, n, k, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0, 1, nullptr};
   int splits = cfg.split_k < 1 ? 1 : cfg.split_k;
   if (splits > 1) {
     int chunk = (k + splits - 1) / splits;
@@ -372,8 +386,13 @@ int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double
       const size_t bytes = (size_t)splits * m * n * sizeof(double);
       double *P = (double *)workspace(cx, WS_MISC, bytes);
       if (!P) return B2_ERR_NOMEM;
+      // arrival counters, one per tile of the finest (64 x 64) tiling
+      const size_t tiles = (size_t)((m + 63) / 64) * ((n + 63) / 64);
+      int *cnt = fixup_counters(cx, tiles, s);
+      if (!cnt) return B2_ERR_NOMEM;
       a.P = P;
       a.ldp = m;
+      a.cnt = cnt;
     } else {
       a.kchunk = k;
     }
@@ -390,13 +409,6 @@ int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double
                   : launch_tile<4, 1>(cfg.tile, ak, bk, a, s);
   }
   if (e != cudaSuccess) return cuda_fail(e, "dgemm_dmma_kernel");
-  if (a.P) {
-    const size_t total = (size_t)m * n;
-    const int blocks = (int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256);
-    B2_PROF("dgemm_splitk_reduce", s);
-    splitk_reduce_kernel<<<blocks, 256, 0, s>>>(m, n, a.splits, a.P, a.ldp, alpha, beta, C, ldc);
-    B2_CUDA_TRY(cudaGetLastError());
-  }
   return B2_OK;
 }
 

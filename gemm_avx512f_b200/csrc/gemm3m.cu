@@ -1,8 +1,9 @@
 // gemm3m.cu -- complex GEMM by the 3M method.
 //
-// Products below 2^24 multiply-adds run in ONE fused launch (below); larger
-// ones run the three real products as the library's own GEMMs between a
-// pre-add pass and a combine pass (gemm3m_three_gemms, at the end).
+// zgemm3m runs in ONE fused launch at every size (zgemm3m_dmma_kernel, FP64
+// DMMA); cgemm3m runs in one fused FFMA launch below 2^24 multiply-adds and
+// otherwise as three 3xTF32 tensor-core GEMMs between a pre-add pass and a
+// combine pass (gemm3m_three_gemms, at the end).
 //
 // Replaces the OpenBLAS gemm3m driver + the reference's 3M kernels
 // (zgemm3m_kernel_2x8_skylakex.c:336-351, zgemm3m_kernel_8x4_skylakex.c:309-334,
@@ -239,6 +240,185 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// --------------------------------------- zgemm3m: one-launch FP64 DMMA --
+// The fused 3M product for complex128 at any size, on the FP64 tensor path
+// (mma.sync.m16n8k8.f64; tcgen05 has no f64 kind).  CTA tile 64 x 64 complex
+// outputs, 16 warps of 16 x 16, K in blocks of 16 complex elements streamed
+// global -> shared by cp.async (one 16-byte complex element per copy, zero
+// filled outside the matrix) through a 4-deep ring.  The smem tile keeps the
+// interleaved (re, im) pairs, so one 16-byte shared load gives a fragment
+// element's real and imaginary part; per K step every warp issues
+//     P1 += Ar Br,   P2 += Ai Bi,   P3 += (Ar + sa Ai)(Br + sb Bi)
+// with the pre-additions made on the fragments in registers (sa, sb = -1 for
+// conjugated operands), and the epilogue forms
+//     Re = P1 - sa sb P2,   Im = P3 - P1 - sa sb P2
+// and applies the complex alpha and beta (beta != 1 scales C, as the
+// reference drivers do: src/gemm_driver.c:131).  Padding: +4 complex per row
+// when K is contiguous, +2 otherwise, so both orientations' 16-byte fragment
+// loads are conflict free.
+constexpr int Z_BM = 64, Z_BN = 64, Z_BK = 16, Z_WM = 4, Z_WN = 4, Z_STAGES = 4;
+constexpr int Z_NT = Z_WM * Z_WN * 32;
+
+template <bool KC>
+__host__ __device__ constexpr int z_stage_elems(int outer) {
+  return KC ? outer * (Z_BK + 4) : Z_BK * (outer + 2);
+}
+
+// One OUTER x BK complex tile; element (o, k) at g[o*ld + k] when KC (K
+// contiguous) else g[k*ld + o] (complex units).  Shared: KC -> [o][BK+4],
+// else [k][OUTER+2].
+template <int OUTER, bool KC>
+__device__ __forceinline__ void z_load_tile(uint32_t sbase, const double2 *__restrict__ g, int ld,
+                                            int o0, int k0, int olim, int klim, int tid) {
+  constexpr int TOTAL = OUTER * Z_BK;
+  static_assert(TOTAL % Z_NT == 0, "tile/thread mismatch");
+#pragma unroll
+  for (int i = 0; i < TOTAL / Z_NT; ++i) {
+    const int c = tid + i * Z_NT;
+    int o, k;
+    if (KC) { o = c / Z_BK; k = c % Z_BK; } else { k = c / OUTER; o = c % OUTER; }
+    const int go = o0 + o, gk = k0 + k;
+    const bool ok = go < olim && gk < klim;
+    const double2 *src = ok ? g + (KC ? (size_t)go * ld + gk : (size_t)gk * ld + go) : g;
+    const uint32_t dst = sbase + (uint32_t)(KC ? o * (Z_BK + 4) + k : k * (OUTER + 2) + o) * 16u;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                 "r"(ok ? 16 : 0));
+  }
+}
+
+template <bool A_KC, bool B_KC>
+__global__ void __launch_bounds__(Z_NT, 1)
+    zgemm3m_dmma_kernel(int M, int N, int K, const double2 *__restrict__ A, int lda,
+                        const double2 *__restrict__ B, int ldb, double2 *__restrict__ C, int ldc,
+                        double ar, double ai, double br, double bi, double sa, double sb) {
+  constexpr int A_ST = z_stage_elems<A_KC>(Z_BM), B_ST = z_stage_elems<B_KC>(Z_BN);
+  extern __shared__ __align__(16) double2 zsh[];
+  double2 *sA = zsh;
+  double2 *sB = zsh + Z_STAGES * A_ST;
+  const uint32_t sA_u = (uint32_t)__cvta_generic_to_shared(sA);
+  const uint32_t sB_u = (uint32_t)__cvta_generic_to_shared(sB);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm0 = (warp / Z_WN) * 16, wn0 = (warp % Z_WN) * 16;
+  const int m0 = blockIdx.x * Z_BM, n0 = blockIdx.y * Z_BN;
+  const int KT = (K + Z_BK - 1) / Z_BK;
+
+  double acc[3][2][4];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[p][j][v] = 0.0;
+
+  auto load_stage = [&](int st, int kt) {
+    const int k0 = kt * Z_BK;
+    z_load_tile<Z_BM, A_KC>(sA_u + st * A_ST * 16, A, lda, m0, k0, M, K, tid);
+    z_load_tile<Z_BN, B_KC>(sB_u + st * B_ST * 16, B, ldb, n0, k0, N, K, tid);
+  };
+#pragma unroll
+  for (int st = 0; st < Z_STAGES - 1; ++st) {
+    if (st < KT) load_stage(st, st);
+    asm volatile("cp.async.commit_group;\n" ::);
+  }
+  for (int kt = 0; kt < KT; ++kt) {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(Z_STAGES - 2));
+    __syncthreads();
+    {
+      const int kn = kt + Z_STAGES - 1;
+      if (kn < KT) load_stage(kn % Z_STAGES, kn);
+      asm volatile("cp.async.commit_group;\n" ::);
+    }
+    const double2 *As = sA + (kt % Z_STAGES) * A_ST;
+    const double2 *Bs = sB + (kt % Z_STAGES) * B_ST;
+#pragma unroll
+    for (int kk = 0; kk < Z_BK; kk += 8) {
+      double are[4], aim[4], bre[2][2], bim[2][2];
+#pragma unroll
+      for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+        for (int v0 = 0; v0 < 2; ++v0) {
+          const int m = wm0 + g + 8 * v0, k = kk + t + 4 * v1;
+          const double2 x = A_KC ? As[m * (Z_BK + 4) + k] : As[k * (Z_BM + 2) + m];
+          are[v0 + 2 * v1] = x.x;
+          aim[v0 + 2 * v1] = x.y;
+        }
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const int n = wn0 + j * 8 + g, k = kk + t + 4 * v;
+          const double2 x = B_KC ? Bs[n * (Z_BK + 4) + k] : Bs[k * (Z_BN + 2) + n];
+          bre[j][v] = x.x;
+          bim[j][v] = x.y;
+        }
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+            "{%8,%9}, {%0,%1,%2,%3};\n"
+            : "+d"(acc[0][j][0]), "+d"(acc[0][j][1]), "+d"(acc[0][j][2]), "+d"(acc[0][j][3])
+            : "d"(are[0]), "d"(are[1]), "d"(are[2]), "d"(are[3]), "d"(bre[j][0]), "d"(bre[j][1]));
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+            "{%8,%9}, {%0,%1,%2,%3};\n"
+            : "+d"(acc[1][j][0]), "+d"(acc[1][j][1]), "+d"(acc[1][j][2]), "+d"(acc[1][j][3])
+            : "d"(aim[0]), "d"(aim[1]), "d"(aim[2]), "d"(aim[3]), "d"(bim[j][0]), "d"(bim[j][1]));
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) are[v] = fma(sa, aim[v], are[v]);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) bre[j][v] = fma(sb, bim[j][v], bre[j][v]);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+            "{%8,%9}, {%0,%1,%2,%3};\n"
+            : "+d"(acc[2][j][0]), "+d"(acc[2][j][1]), "+d"(acc[2][j][2]), "+d"(acc[2][j][3])
+            : "d"(are[0]), "d"(are[1]), "d"(are[2]), "d"(are[3]), "d"(bre[j][0]), "d"(bre[j][1]));
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::);
+
+  // Fragment (j, v): row g + 8 (v >> 1), column 2t + (v & 1) of the warp tile.
+  const double s2 = sa * sb;
+  const bool beta_one = br == 1.0 && bi == 0.0;
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int m = m0 + wm0 + g + 8 * (v >> 1);
+      const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
+      if (m < M && n < N) {
+        const double p1 = acc[0][j][v], p2 = s2 * acc[1][j][v], p3 = acc[2][j][v];
+        const double re = p1 - p2, im = p3 - p1 - p2;
+        double2 *c = C + (size_t)n * ldc + m;
+        double2 cv = *c;
+        if (!beta_one) cv = make_double2(br * cv.x - bi * cv.y, br * cv.y + bi * cv.x);
+        *c = make_double2(cv.x + (ar * re - ai * im), cv.y + (ar * im + ai * re));
+      }
+    }
+}
+
+template <bool AK, bool BKc>
+int launch_zgemm3m_dmma(int m, int n, int k, const double *A, int lda, const double *B, int ldb,
+                        double *C, int ldc, double ar, double ai, double br, double bi, double sa,
+                        double sb, cudaStream_t s) {
+  constexpr size_t SMEM =
+      (size_t)Z_STAGES * (z_stage_elems<AK>(Z_BM) + z_stage_elems<BKc>(Z_BN)) * 16;
+  auto kern = zgemm3m_dmma_kernel<AK, BKc>;
+  B2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM));
+  dim3 grid((unsigned)((m + Z_BM - 1) / Z_BM), (unsigned)((n + Z_BN - 1) / Z_BN));
+  B2_PROF("zgemm3m_dmma", s);
+  kern<<<grid, Z_NT, SMEM, s>>>(m, n, k, reinterpret_cast<const double2 *>(A), lda,
+                                reinterpret_cast<const double2 *>(B), ldb,
+                                reinterpret_cast<double2 *>(C), ldc, ar, ai, br, bi, sa, sb);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
 template <typename T>
 __global__ void cscale_kernel(int M, int N, T br, T bi, T *__restrict__ C, int ldc) {
   const long long total = (long long)M * N;
@@ -346,6 +526,25 @@ int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T
     cscale_kernel<T><<<blocks, 256, 0, s>>>(m, n, br, bi, C, ldc);
     B2_CUDA_TRY(cudaGetLastError());
     return B2_OK;
+  }
+  if constexpr (sizeof(T) == 8) {
+    // complex128: the one-launch DMMA kernel at every size (16-byte aligned
+    // operands, the normal case; an odd-aligned pointer takes the other paths)
+    const bool al16 = (((uintptr_t)A | (uintptr_t)B | (uintptr_t)C) & 15) == 0;
+    if (al16) {
+      const bool tA = !(ta == 'N' || ta == 'n' || ta == 'R' || ta == 'r');
+      const bool tB = !(tb == 'N' || tb == 'n' || tb == 'R' || tb == 'r');
+      const double sA = (ta == 'C' || ta == 'c' || ta == 'R' || ta == 'r') ? -1.0 : 1.0;
+      const double sB = (tb == 'C' || tb == 'c' || tb == 'R' || tb == 'r') ? -1.0 : 1.0;
+      const bool ak = tA, bk = !tB;  // K contiguous in memory
+      if (ak && bk)
+        return launch_zgemm3m_dmma<true, true>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, sA, sB, s);
+      if (ak)
+        return launch_zgemm3m_dmma<true, false>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, sA, sB, s);
+      if (bk)
+        return launch_zgemm3m_dmma<false, true>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, sA, sB, s);
+      return launch_zgemm3m_dmma<false, false>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, sA, sB, s);
+    }
   }
   if ((double)m * n * k >= 16777216.0)
     return gemm3m_three_gemms<T>(ta, tb, m, n, k, ar, ai, br, bi, A, lda, B, ldb, C, ldc, s);

@@ -9,7 +9,7 @@
 // persistent grid pulls tile indices from a device-side atomic counter, finds
 // the owning problem by binary search over the tile prefix sums and runs the
 // tile with the problem's own dtype, transposes, strides and alpha/beta:
-//   FP64 tiles: DMMA mma.sync.m16n8k4.f64, 8 warps of 32 x 16;
+//   FP64 tiles: DMMA mma.sync.m16n8k8.f64, 8 warps of 32 x 16;
 //   FP32 tiles: FFMA, 256 threads of 4 x 4.
 // A plan uploads the descriptors once and captures "reset counter + launch" in
 // a CUDA graph, so replaying a batch is a single graph launch.
@@ -127,25 +127,32 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+  // DMMA m16n8k8: A fragment rows g, g+8 x k t, t+4; B fragment k t, t+4 x column g
   tile_k_loop<double>(g, m0, n0, sm, [&](const double *As, const double *Bs) {
 #pragma unroll
-    for (int kk = 0; kk < GT_K; kk += 4) {
-      double af[2][2], bf[2];
+    for (int kk = 0; kk < GT_K; kk += 8) {
+      double af[2][4], bf[2][2];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int v = 0; v < 2; ++v) af[i][v] = As[(kk + t) * GT_LD + wm0 + i * 16 + gq + 8 * v];
+        for (int v1 = 0; v1 < 2; ++v1)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) bf[j] = Bs[(kk + t) * GT_LD + wn0 + j * 8 + gq];
+          for (int v0 = 0; v0 < 2; ++v0)
+            af[i][v0 + 2 * v1] = As[(kk + t + 4 * v1) * GT_LD + wm0 + i * 16 + gq + 8 * v0];
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) bf[j][v] = Bs[(kk + t + 4 * v) * GT_LD + wn0 + j * 8 + gq];
 #pragma unroll
       for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < 2; ++j)
           asm volatile(
-              "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
-              "{%0,%1,%2,%3};\n"
+              "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+              "{%8,%9}, {%0,%1,%2,%3};\n"
               : "+d"(acc[i][j][0]), "+d"(acc[i][j][1]), "+d"(acc[i][j][2]), "+d"(acc[i][j][3])
-              : "d"(af[i][0]), "d"(af[i][1]), "d"(bf[j]));
+              : "d"(af[i][0]), "d"(af[i][1]), "d"(af[i][2]), "d"(af[i][3]), "d"(bf[j][0]),
+                "d"(bf[j][1]));
     }
   });
   double *C = (double *)g.C;
@@ -199,7 +206,7 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
     }
 }
 
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
     grouped_kernel(const GroupDesc *__restrict__ d, int count, long long total_tiles,
                    unsigned long long *counter) {
   __shared__ __align__(16) double sm[2 * GT_STAGE];  // two stages of A and B panels

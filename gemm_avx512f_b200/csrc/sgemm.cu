@@ -3,101 +3,188 @@
 // Native FP32 replaces the reference's AVX-512 SGEMM (src/gemm_driver.c:116
 // built without -DDOUBLE driving the 48x8 tile of src/kernel/gemm_kernel.S,
 // and the m16 x n24 tiles of OpenBLAS-like_implementation/sgemm.c:366-412):
-// a CUDA-core FFMA kernel with a 128x128 CTA tile, 8x8 outputs per thread in
-// registers, double-buffered shared-memory K panels.  The tensor-core forms
-// (TF32, 3xTF32, 3xBF16) run on the tcgen05 engine in umma_gemm.cu.
+// a CUDA-core kernel of paired FP32 FMAs (fma.rn.f32x2) with a 128x128 CTA
+// tile, 8x8 outputs per thread in registers, double-buffered shared-memory K
+// panels.  The tensor-core forms (TF32, 3xTF32, 3xBF16) run on the tcgen05
+// engine (sgemm_tc.cu).
 #include "b2_methods.cuh"
 #include "b2_profile.cuh"
 
 namespace b2 {
 namespace {
 
-constexpr int SB_M = 128, SB_N = 128, SB_K = 8, SB_PAD = 4;
+// ----------------------------------------------------------------------
+// Paired-FMA FP32 kernel (sm_100 fma.rn.f32x2: two FP32 FMAs per issued
+// instruction, so the FFMA pipe, not instruction issue, is the limit).
+// CTA tile 128 x 128, K blocks of 16, 256 threads of 8 x 8 outputs, K panels
+// staged through registers (16-byte global loads when the layout allows)
+// into double-buffered shared memory.  A is stored in shared memory with every
+// value duplicated, (a, a), so one 16-byte shared load yields the two
+// broadcast pairs that multiply a pair of B values; thread (tx, ty) owns rows
+// 2 tx + {0, 1} + 32 q (q = 0..3: conflict-free 16-byte loads across the
+// half-warp) and columns 4 ty + {0..3} + 64 h (h = 0, 1).
+constexpr int S2_M = 128, S2_N = 128, S2_K = 16, S2_APAD = 4, S2_BPAD = 4;
+constexpr int S2_ALD = 2 * S2_M + S2_APAD;  // floats per k row of the duplicated A panel
+constexpr int S2_BLD = S2_N + S2_BPAD;
+constexpr int S2_SMEM = (2 * S2_K * S2_ALD + 2 * S2_K * S2_BLD) * 4;
 
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(256, 2)
-    sgemm_simt_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, int lda,
-                      const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
-                      int ldc) {
-  __shared__ __align__(16) float As[2][SB_K][SB_M + SB_PAD];
-  __shared__ __align__(16) float Bs[2][SB_K][SB_N + SB_PAD];
-  const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-  const int m0 = blockIdx.x * SB_M, n0 = blockIdx.y * SB_N;
-  float acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+__device__ __forceinline__ void ffma2(unsigned long long &c, unsigned long long a,
+                                      unsigned long long b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(c) : "l"(a), "l"(b));
+}
 
-  float ra[4], rb[4];
+// Four consecutive floats starting at p (16-byte aligned when VEC), or fewer
+// at the matrix edge (lim = elements available from p), zero beyond.
+template <bool VEC>
+__device__ __forceinline__ float4 load4(const float *p, int lim) {
+  if (VEC && lim >= 4) return __ldg(reinterpret_cast<const float4 *>(p));
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (lim > 0) v.x = p[0];
+  if (lim > 1) v.y = p[1];
+  if (lim > 2) v.z = p[2];
+  if (lim > 3) v.w = p[3];
+  return v;
+}
+
+template <bool TA, bool TB, bool VEC>
+__global__ void __launch_bounds__(256, 1)
+    sgemm_ffma2_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, int lda,
+                       const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
+                       int ldc) {
+  extern __shared__ __align__(16) float s2mem[];
+  float *As = s2mem;                        // [2][S2_K][S2_ALD] duplicated pairs
+  float *Bs = s2mem + 2 * S2_K * S2_ALD;    // [2][S2_K][S2_BLD]
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * S2_M, n0 = blockIdx.y * S2_N;
+
+  unsigned long long acc[8][4];  // row r: 2tx + (r&1) + 32(r>>1); column pair c
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0ull;
+
+  // Register staging of one K block: 8 A values and 8 B values per thread.
+  // A: element (m, k) at A[k*lda + m] ('N') or A[m*lda + k] ('T');
+  // B: element (k, n) at B[n*ldb + k] ('N') or B[k*ldb + n] ('T').
+  float4 ra[2], rb[2];
   auto gload = [&](int k0) {
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int idx = tid + 256 * e;
-      int kk, mm;
-      if (TA) { kk = idx % SB_K; mm = idx / SB_K; } else { kk = idx / SB_M; mm = idx % SB_M; }
-      const int gm = m0 + mm, gk = k0 + kk;
-      ra[e] = (gm < M && gk < K) ? (TA ? A[(size_t)gm * lda + gk] : A[(size_t)gk * lda + gm]) : 0.f;
-      int nn;
-      if (!TB) { kk = idx % SB_K; nn = idx / SB_K; } else { kk = idx / SB_N; nn = idx % SB_N; }
-      const int gn = n0 + nn, gk2 = k0 + kk;
-      rb[e] = (gn < N && gk2 < K) ? (TB ? B[(size_t)gk2 * ldb + gn] : B[(size_t)gn * ldb + gk2]) : 0.f;
+    for (int h = 0; h < 2; ++h) {
+      const int c = tid + 256 * h;
+      if (!TA) {  // 4 consecutive m of one k
+        const int kk = c >> 5, mm = (c & 31) * 4, gm = m0 + mm, gk = k0 + kk;
+        ra[h] = gk < K ? load4<VEC>(A + (size_t)gk * lda + gm, M - gm) : make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {    // 4 consecutive k of one m
+        const int mm = c >> 2, kk = (c & 3) * 4, gm = m0 + mm, gk = k0 + kk;
+        ra[h] = gm < M ? load4<VEC>(A + (size_t)gm * lda + gk, K - gk) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      if (TB) {   // 4 consecutive n of one k
+        const int kk = c >> 5, nn = (c & 31) * 4, gn = n0 + nn, gk = k0 + kk;
+        rb[h] = gk < K ? load4<VEC>(B + (size_t)gk * ldb + gn, N - gn) : make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {    // 4 consecutive k of one n
+        const int nn = c >> 2, kk = (c & 3) * 4, gn = n0 + nn, gk = k0 + kk;
+        rb[h] = gn < N ? load4<VEC>(B + (size_t)gn * ldb + gk, K - gk) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
   };
   auto sstore = [&](int buf) {
+    float *as = As + buf * S2_K * S2_ALD;
+    float *bs = Bs + buf * S2_K * S2_BLD;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int idx = tid + 256 * e;
-      int kk, mm;
-      if (TA) { kk = idx % SB_K; mm = idx / SB_K; } else { kk = idx / SB_M; mm = idx % SB_M; }
-      As[buf][kk][mm] = ra[e];
-      int nn;
-      if (!TB) { kk = idx % SB_K; nn = idx / SB_K; } else { kk = idx / SB_N; nn = idx % SB_N; }
-      Bs[buf][kk][nn] = rb[e];
+    for (int h = 0; h < 2; ++h) {
+      const int c = tid + 256 * h;
+      const float av[4] = {ra[h].x, ra[h].y, ra[h].z, ra[h].w};
+      if (!TA) {  // two 16-byte stores of duplicated pairs
+        const int kk = c >> 5, mm = (c & 31) * 4;
+        float *d = as + kk * S2_ALD + 2 * mm;
+        *reinterpret_cast<float4 *>(d) = make_float4(av[0], av[0], av[1], av[1]);
+        *reinterpret_cast<float4 *>(d + 4) = make_float4(av[2], av[2], av[3], av[3]);
+      } else {
+        const int mm = c >> 2, kk = (c & 3) * 4;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          *reinterpret_cast<float2 *>(as + (kk + e) * S2_ALD + 2 * mm) = make_float2(av[e], av[e]);
+      }
+      if (TB) {
+        const int kk = c >> 5, nn = (c & 31) * 4;
+        *reinterpret_cast<float4 *>(bs + kk * S2_BLD + nn) = rb[h];
+      } else {
+        const int nn = c >> 2, kk = (c & 3) * 4;
+        const float bv[4] = {rb[h].x, rb[h].y, rb[h].z, rb[h].w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) bs[(kk + e) * S2_BLD + nn] = bv[e];
+      }
     }
   };
 
-  const int KT = (K + SB_K - 1) / SB_K;
+  const int KT = (K + S2_K - 1) / S2_K;
   gload(0);
   sstore(0);
   __syncthreads();
   for (int kt = 0; kt < KT; ++kt) {
     const int buf = kt & 1;
-    if (kt + 1 < KT) gload((kt + 1) * SB_K);
+    if (kt + 1 < KT) gload((kt + 1) * S2_K);
+    const float *as = As + buf * S2_K * S2_ALD;
+    const float *bs = Bs + buf * S2_K * S2_BLD;
 #pragma unroll
-    for (int kk = 0; kk < SB_K; ++kk) {
-      float a[8], b[8];
-      const float4 a0 = *reinterpret_cast<const float4 *>(&As[buf][kk][tx * 4]);
-      const float4 a1 = *reinterpret_cast<const float4 *>(&As[buf][kk][64 + tx * 4]);
-      const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][ty * 4]);
-      const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[buf][kk][64 + ty * 4]);
-      a[0] = a0.x; a[1] = a0.y; a[2] = a0.z; a[3] = a0.w;
-      a[4] = a1.x; a[5] = a1.y; a[6] = a1.z; a[7] = a1.w;
-      b[0] = b0.x; b[1] = b0.y; b[2] = b0.z; b[3] = b0.w;
-      b[4] = b1.x; b[5] = b1.y; b[6] = b1.z; b[7] = b1.w;
+    for (int kk = 0; kk < S2_K; ++kk) {
+      ulonglong2 a2[4];  // duplicated pairs of rows 32q + 2tx and 32q + 2tx + 1
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int q = 0; q < 4; ++q)
+        a2[q] = *reinterpret_cast<const ulonglong2 *>(as + kk * S2_ALD + 2 * (32 * q + 2 * tx));
+      ulonglong2 b2[2];  // columns 64h + 4ty .. 64h + 4ty + 3
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+      for (int h = 0; h < 2; ++h)
+        b2[h] = *reinterpret_cast<const ulonglong2 *>(bs + kk * S2_BLD + 64 * h + 4 * ty);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          ffma2(acc[2 * q][2 * h], a2[q].x, b2[h].x);
+          ffma2(acc[2 * q][2 * h + 1], a2[q].x, b2[h].y);
+          ffma2(acc[2 * q + 1][2 * h], a2[q].y, b2[h].x);
+          ffma2(acc[2 * q + 1][2 * h + 1], a2[q].y, b2[h].y);
+        }
+      }
     }
     if (kt + 1 < KT) {
+      // the other buffer was last read in the previous iteration, which every
+      // thread finished before that iteration's closing barrier
       sstore(buf ^ 1);
       __syncthreads();
     }
   }
   const bool beta_one = (beta == 1.f);
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int n = n0 + (j < 4 ? ty * 4 + j : 64 + ty * 4 + (j - 4));
-    if (n >= N) continue;
+  for (int r = 0; r < 8; ++r) {
+    const int m = m0 + 2 * tx + (r & 1) + 32 * (r >> 1);
+    if (m >= M) continue;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int m = m0 + (i < 4 ? tx * 4 + i : 64 + tx * 4 + (i - 4));
-      if (m >= M) continue;
-      float *p = C + (size_t)n * ldc + m;
-      *p = beta_one ? fmaf(alpha, acc[i][j], *p) : fmaf(alpha, acc[i][j], beta * *p);
+    for (int c = 0; c < 4; ++c) {
+      const float2 v = *reinterpret_cast<const float2 *>(&acc[r][c]);
+      const int nb = n0 + 64 * (c >> 1) + 4 * ty + 2 * (c & 1);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int n = nb + e;
+        if (n >= N) continue;
+        float *p = C + (size_t)n * ldc + m;
+        const float x = e ? v.y : v.x;
+        *p = beta_one ? fmaf(alpha, x, *p) : fmaf(alpha, x, beta * *p);
+      }
     }
   }
+}
+
+template <bool TA, bool TB, bool VEC>
+int launch_ffma2(int m, int n, int k, float alpha, const float *A, int lda, const float *B,
+                 int ldb, float beta, float *C, int ldc, cudaStream_t s) {
+  auto kern = sgemm_ffma2_kernel<TA, TB, VEC>;
+  B2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM));
+  dim3 grid((m + S2_M - 1) / S2_M, (n + S2_N - 1) / S2_N);
+  B2_PROF("sgemm_simt", s);
+  kern<<<grid, 256, S2_SMEM, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
 }
 
 }  // namespace
@@ -108,18 +195,19 @@ int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *
   if (k <= 0 || alpha == 0.f) return beta == 1.f ? B2_OK : scale_matrix_s(m, n, beta, C, ldc, s);
   const bool TA = !(ta == 'N' || ta == 'n');
   const bool TB = !(tb == 'N' || tb == 'n');
-  dim3 grid((m + SB_M - 1) / SB_M, (n + SB_N - 1) / SB_N);
-  B2_PROF("sgemm_simt", s);
-  if (TA && TB)
-    sgemm_simt_kernel<true, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  else if (TA)
-    sgemm_simt_kernel<true, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  else if (TB)
-    sgemm_simt_kernel<false, true><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  else
-    sgemm_simt_kernel<false, false><<<grid, 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  B2_CUDA_TRY(cudaGetLastError());
-  return B2_OK;
+  // 16-byte loads need 16-byte aligned bases and leading dimensions of 4k floats
+  const bool vec = (lda % 4 == 0) && (ldb % 4 == 0) && (((uintptr_t)A & 15) == 0) &&
+                   (((uintptr_t)B & 15) == 0);
+  if (vec) {
+    if (TA && TB) return launch_ffma2<true, true, true>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    if (TA) return launch_ffma2<true, false, true>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    if (TB) return launch_ffma2<false, true, true>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+    return launch_ffma2<false, false, true>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+  }
+  if (TA && TB) return launch_ffma2<true, true, false>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+  if (TA) return launch_ffma2<true, false, false>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+  if (TB) return launch_ffma2<false, true, false>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
+  return launch_ffma2<false, false, false>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, s);
 }
 
 int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,

@@ -58,6 +58,11 @@ def to_dev(x, cuda):
 
 
 def from_dev(t):
+    """Host copy once every stream has finished (the library's default stream
+    is a non-blocking stream, which torch's copy would not wait for)."""
+    import torch
+
+    torch.cuda.synchronize()
     return np.asfortranarray(t.cpu().numpy().T)
 
 
