@@ -1097,7 +1097,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   // auxiliary stream, so most of the auxiliary passes hide under the GEMMs.
   const int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
                  (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
-                    ? (n / 2048 < 2 ? 2 : (n / 2048 > 8 ? 8 : n / 2048))
+                    ? (n / 1024 < 2 ? 2 : (n / 1024 > 8 ? 8 : n / 1024))
                     : 1;
   if (J > 1) {
     const int nb = (int)round_up((n + J - 1) / J, 256);

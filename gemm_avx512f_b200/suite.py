@@ -46,7 +46,7 @@ import time
 
 import numpy as np
 
-from . import _lib, blas
+from . import _lib, blas, inputs
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SM = 148
@@ -87,6 +87,15 @@ class Timer:
         return e0.elapsed_time(e1) / reps
 
 
+def upload(x, dev):
+    """A Fortran-ordered host matrix as a flat column-major device tensor."""
+    import torch
+
+    t = torch.from_numpy(np.asfortranarray(x).reshape(-1, order="F")).to(dev)
+    torch.cuda.synchronize()
+    return t
+
+
 def emit(out, rec):
     line = json.dumps(rec)
     print(line, flush=True)
@@ -99,10 +108,7 @@ def run_dgemm(ctx, out, quick):
     torch, dev, T, P = ctx["torch"], ctx["dev"], ctx["timer"], ctx["peaks"]
     st = ctx["stream"]
     n = 1024
-    g = torch.Generator(device=dev)
-    g.manual_seed(0)
-    A, B, C0 = (torch.rand(n * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1
-                for _ in range(3))
+    A, B, C0 = (upload(x, dev) for x in inputs.config1(n))
     blas.load_selector()
     for method in ("fp64", "ozaki", "auto"):
         Cm = C0.clone()
@@ -130,16 +136,15 @@ def run_sgemm(ctx, out, quick):
         shapes = [(4096, 4096, 4096), (8192, 256, 8192)]
     if ctx.get("sgemm_shapes"):
         shapes = ctx["sgemm_shapes"]
-    g = torch.Generator(device=dev)
-    g.manual_seed(1)
     bound = {"fp32": ("fp32 SIMT (nominal)", P["fp32_tflops"], 1),
              "tf32": ("tf32 tensor", P["tf32_tflops"], 1),
              "tf32x3": ("tf32 tensor, 3 MMAs per product", P["tf32_tflops"], 3),
              "bf16x3": ("bf16 tensor, 3 MMAs per product", P["bf16_tflops"], 3)}
     for (m, n, k) in shapes:
         for ta, tb in (("N", "N"), ("N", "T"), ("T", "N"), ("T", "T")):
-            A = torch.rand(m * k, dtype=torch.float32, device=dev, generator=g) * 2 - 1
-            B = torch.rand(k * n, dtype=torch.float32, device=dev, generator=g) * 2 - 1
+            ha, hb = inputs.config2(m, n, k, ta, tb)
+            A, B = upload(ha, dev), upload(hb, dev)
+            del ha, hb
             lda, ldb = (m if ta == "N" else k), (k if tb == "N" else n)
             Am = A.view(-1, lda).t()  # column-major lda x cols
             Bm = B.view(-1, ldb).t()
@@ -168,12 +173,9 @@ def run_ozaki(ctx, out, quick):
     sizes = [4096, 8192, 16384] if not quick else [4096]
     for n in sizes:
         for phi in (0.1, 1.0, 4.0):
-            g = torch.Generator(device=dev)
-            g.manual_seed(2)
-            A = ((torch.rand(n * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1) *
-                 torch.exp(phi * torch.randn(n * n, dtype=torch.float64, device=dev, generator=g)))
-            B = ((torch.rand(n * n, dtype=torch.float64, device=dev, generator=g) * 2 - 1) *
-                 torch.exp(phi * torch.randn(n * n, dtype=torch.float64, device=dev, generator=g)))
+            ha, hb = inputs.config3(n, phi)
+            A, B = upload(ha, dev), upload(hb, dev)
+            del ha, hb
             res, moduli = {}, 0
             for method in ("ozaki", "fp64"):
                 Cm = torch.zeros(n * n, dtype=torch.float64, device=dev)
@@ -206,17 +208,15 @@ def run_grouped(ctx, out, quick):
     torch, dev, T = ctx["torch"], ctx["dev"], ctx["timer"]
     st = ctx["stream"]
     L = _lib.lib()
-    rng = np.random.default_rng(3)
     count = 4096
     probs, keep, flops = [], [], 0.0
-    for i in range(count):
-        m, n, k = (int(round(np.exp(rng.uniform(np.log(16), np.log(1024))))) for _ in range(3))
-        dt = i % 2
-        ta, tb = ("N", "T")[rng.integers(2)], ("N", "T")[rng.integers(2)]
+    for i, (dt, ta, tb, m, n, k) in enumerate(inputs.config4_problems(count)):
+        rng = np.random.default_rng([3, i])
+        npdt = np.float64 if dt == 0 else np.float32
         tdt = torch.float64 if dt == 0 else torch.float32
         ar, br = (m if ta == "N" else k), (k if tb == "N" else n)
-        A = torch.rand(m * k, dtype=tdt, device=dev) * 2 - 1
-        B = torch.rand(k * n, dtype=tdt, device=dev) * 2 - 1
+        A = upload(rng.uniform(-1, 1, (ar, m * k // ar)).astype(npdt), dev)
+        B = upload(rng.uniform(-1, 1, (br, k * n // br)).astype(npdt), dev)
         Cm = torch.zeros(m * n, dtype=tdt, device=dev)
         probs.append(_lib.GemmProblem(dt, ta.encode(), tb.encode(), m, n, k, 1.0, 0.0,
                                       A.data_ptr(), ar, B.data_ptr(), br, Cm.data_ptr(), m))
@@ -250,14 +250,9 @@ def run_complex(ctx, out, quick):
     torch, dev, T, P = ctx["torch"], ctx["dev"], ctx["timer"], ctx["peaks"]
     st = ctx["stream"]
     n = 2048
-    g = torch.Generator(device=dev)
-    g.manual_seed(3)
-
-    def cplx(dt):
-        return torch.complex(torch.rand(n * n, dtype=dt, device=dev, generator=g) * 2 - 1,
-                             torch.rand(n * n, dtype=dt, device=dev, generator=g) * 2 - 1)
-
-    A, B = cplx(torch.float64), cplx(torch.float64)
+    ha, hb, _ = inputs.config4_complex(n)
+    A, B = upload(ha, dev), upload(hb, dev)
+    del ha, hb
     ref = A.view(n, n).t() @ B.view(n, n).t()
     for name, fn, dt in (("zgemm3m", blas.zgemm3m_device, torch.complex128),
                          ("cgemm3m", blas.cgemm3m_device, torch.complex64)):
@@ -282,12 +277,11 @@ def run_trsm(ctx, out, quick):
     torch, dev, T, P = ctx["torch"], ctx["dev"], ctx["timer"], ctx["peaks"]
     st = ctx["stream"]
     n, nrhs = (16384, 4096) if not quick else (8192, 2048)
-    g = torch.Generator(device=dev)
-    g.manual_seed(4)
-    Lm = torch.tril(torch.rand((n, n), dtype=torch.float64, device=dev, generator=g) * 2 - 1)
-    Lm.diagonal().copy_(n + torch.rand(n, dtype=torch.float64, device=dev, generator=g))
-    Acm = Lm.t().contiguous()  # column-major storage of L
-    B0 = torch.rand((nrhs, n), dtype=torch.float64, device=dev, generator=g) * 2 - 1
+    ha, hb = inputs.config5(n, nrhs)
+    Acm = upload(ha, dev)  # column-major storage of the lower triangle L
+    Lm = Acm.view(n, n).t()
+    B0 = upload(hb, dev).view(nrhs, n)
+    del ha, hb
     for upd in ("fp64", "ozaki"):
         X = B0.clone()
 
