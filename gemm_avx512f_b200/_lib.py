@@ -115,6 +115,9 @@ def lib() -> C.CDLL:
     L.b2_tune_config_count.restype = i
     L.b2_mlp_param_count.restype = i
     L.b2_dgemm_config.argtypes = [ch, ch, i, i, i, d, p, i, p, i, d, p, i, i, p]
+    L.b2_sgemm_config.argtypes = [ch, ch, i, i, i, f, p, i, p, i, f, p, i, i, p]
+    L.b2_tune_sweep_sgemm.argtypes = [i, p, i, p]
+    L.b2_sgemm_selector_choose.argtypes = [i, ch, ch, i, i, i, i]
     L.b2_tune_sweep.argtypes = [i, p, i, p]
     L.b2_mlp_train.argtypes = [i, p, p, i, i, f, i, p, p, p]
     L.b2_mlp_forward.argtypes = [p, i, p, p]
@@ -122,7 +125,8 @@ def lib() -> C.CDLL:
     L.b2_selector_set.argtypes = [p]
     L.b2_selector_choose.argtypes = [ch, ch, i, i, i, i, i]
     L.b2_selector_predict.argtypes = [ch, ch, i, i, i, i, p]
-    for nm in ("b2_dgemm_config", "b2_tune_sweep", "b2_mlp_train", "b2_mlp_forward",
+    for nm in ("b2_dgemm_config", "b2_tune_sweep", "b2_sgemm_config", "b2_tune_sweep_sgemm",
+               "b2_sgemm_selector_choose", "b2_mlp_train", "b2_mlp_forward",
                "b2_mlp_gradient", "b2_selector_set", "b2_selector_choose", "b2_selector_predict"):
         getattr(L, nm).restype = i
     L.b2_set_fp64_config.argtypes = [i, i, i]

@@ -59,6 +59,10 @@ struct CtxOwner {
       if (c->ev_c[i]) cudaEventDestroy(c->ev_c[i]);
     }
     if (c->plan_ev) cudaEventDestroy(c->plan_ev);
+    for (int i = 0; i < 2; ++i) {
+      if (c->bounce_ev[i]) cudaEventSynchronize(c->bounce_ev[i]), cudaEventDestroy(c->bounce_ev[i]);
+      if (c->bounce[i]) cudaFreeHost(c->bounce[i]);
+    }
     for (int i = 0; i < Ctx::OZ_EVENTS; ++i)
       if (c->oz_ev[i]) cudaEventDestroy(c->oz_ev[i]);
     if (c->oz_gemm) cudaStreamSynchronize(c->oz_gemm), cudaStreamDestroy(c->oz_gemm);
@@ -237,25 +241,201 @@ bool is_device_ptr(const void *p) {
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
 }
 
+// ------------------------------------------------ pageable host buffers --
+// A reference BLAS caller passes malloc'ed (pageable) memory.  The CUDA
+// driver copies such memory through its own staging with one host thread,
+// about 10 GB/s here; instead the library copies it through two pinned
+// bounce buffers of its own, with up to 16 host threads doing the host-side
+// copy of one buffer while the DMA engine moves the other.
+bool host_pageable(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { (void)cudaGetLastError(); return true; }
+  return at.type == cudaMemoryTypeUnregistered;
+}
+
+namespace {
+// Persistent host threads that run the tasks of one parallel copy; the
+// calling thread takes tasks too.  One parallel copy at a time.
+struct CopyPool {
+  std::mutex run_mu, mu;
+  std::condition_variable cv, cv_done;
+  const std::function<void(int)> *job = nullptr;
+  int ntasks = 0, next = 0, pending = 0;
+  unsigned long gen = 0;
+  int workers = -1;
+
+  void worker() {
+    unsigned long seen = 0;
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      cv.wait(lk, [&] { return gen != seen; });
+      seen = gen;
+      while (job && next < ntasks) {
+        const int t = next++;
+        const std::function<void(int)> *f = job;
+        lk.unlock();
+        (*f)(t);
+        lk.lock();
+        if (--pending == 0) cv_done.notify_all();
+      }
+    }
+  }
+  void run(int n, const std::function<void(int)> &f) {
+    std::lock_guard<std::mutex> rl(run_mu);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (workers < 0) {
+        unsigned hw = std::thread::hardware_concurrency();
+        workers = (int)(hw > 16 ? 15 : (hw > 1 ? hw - 1 : 0));
+        for (int i = 0; i < workers; ++i) {
+          try {
+            std::thread([this] { worker(); }).detach();
+          } catch (...) {
+            workers = i;
+            break;
+          }
+        }
+      }
+    }
+    std::unique_lock<std::mutex> lk(mu);
+    job = &f;
+    ntasks = n;
+    next = 0;
+    pending = n;
+    ++gen;
+    cv.notify_all();
+    while (next < ntasks) {
+      const int t = next++;
+      lk.unlock();
+      f(t);
+      lk.lock();
+      --pending;
+    }
+    cv_done.wait(lk, [&] { return pending == 0; });
+    job = nullptr;
+  }
+};
+CopyPool g_copy_pool;
+
+// rows x width bytes from src (pitch spitch) to dst (pitch dpitch), split over
+// the pool when large.
+void parallel_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                     size_t rows) {
+  const size_t total = width * rows;
+  const int tasks = total < (size_t)(4u << 20) ? 1 : 16;
+  auto body = [&](int t) {
+    const size_t r0 = rows * t / tasks, r1 = rows * (t + 1) / tasks;
+    for (size_t r = r0; r < r1; ++r)
+      memcpy((char *)dst + r * dpitch, (const char *)src + r * spitch, width);
+  };
+  if (tasks == 1) {
+    body(0);
+    return;
+  }
+  const std::function<void(int)> f = body;
+  g_copy_pool.run(tasks, f);
+}
+
+int bounce_ready(Ctx *c) {
+  for (int i = 0; i < 2; ++i) {
+    if (!c->bounce[i] && cudaMallocHost(&c->bounce[i], Ctx::BOUNCE_BYTES) != cudaSuccess) {
+      (void)cudaGetLastError();
+      c->bounce[i] = nullptr;
+      return B2_ERR_NOMEM;
+    }
+    if (!c->bounce_ev[i] &&
+        cudaEventCreateWithFlags(&c->bounce_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+      (void)cudaGetLastError();
+      c->bounce_ev[i] = nullptr;
+      return B2_ERR_CUDA;
+    }
+  }
+  return B2_OK;
+}
+}  // namespace
+
+// Host -> device 2-D copy (rows of `width` bytes), stream-ordered on s; a
+// pageable source goes through the bounce buffers (the call returns once the
+// host side has been copied; the DMAs stay queued on s).
+int copy_h2d(Ctx *c, void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+             size_t rows, cudaStream_t s) {
+  if (!rows || !width) return B2_OK;
+  if (!host_pageable(src) || width > Ctx::BOUNCE_BYTES) {
+    B2_CUDA_TRY(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDefault, s));
+    return B2_OK;
+  }
+  int rc = bounce_ready(c);
+  if (rc != B2_OK) return rc;
+  const size_t per = Ctx::BOUNCE_BYTES / width;
+  for (size_t r0 = 0, i = 0; r0 < rows; r0 += per, ++i) {
+    const size_t nr = rows - r0 < per ? rows - r0 : per;
+    const int slot = (int)(i & 1);
+    B2_CUDA_TRY(cudaEventSynchronize(c->bounce_ev[slot]));  // its previous DMA has finished
+    parallel_copy2d(c->bounce[slot], width, (const char *)src + r0 * spitch, spitch, width, nr);
+    B2_CUDA_TRY(cudaMemcpy2DAsync((char *)dst + r0 * dpitch, dpitch, c->bounce[slot], width, width,
+                                  nr, cudaMemcpyHostToDevice, s));
+    B2_CUDA_TRY(cudaEventRecord(c->bounce_ev[slot], s));
+  }
+  return B2_OK;
+}
+
+// Device -> host 2-D copy after the work queued on s; synchronous (the data
+// is in host memory on return).  A pageable destination is filled from the
+// bounce buffers, the DMA of the next chunk overlapping the host-side copy.
+int copy_d2h(Ctx *c, void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+             size_t rows, cudaStream_t s) {
+  if (!rows || !width) return B2_OK;
+  if (!host_pageable(dst) || width > Ctx::BOUNCE_BYTES) {
+    B2_CUDA_TRY(cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, cudaMemcpyDefault, s));
+    B2_CUDA_TRY(cudaStreamSynchronize(s));
+    return B2_OK;
+  }
+  int rc = bounce_ready(c);
+  if (rc != B2_OK) return rc;
+  const size_t per = Ctx::BOUNCE_BYTES / width;
+  const size_t nchunks = (rows + per - 1) / per;
+  auto issue = [&](size_t i) -> cudaError_t {
+    const size_t r0 = i * per, nr = rows - r0 < per ? rows - r0 : per;
+    const int slot = (int)(i & 1);
+    cudaError_t e = cudaEventSynchronize(c->bounce_ev[slot]);
+    if (e == cudaSuccess)
+      e = cudaMemcpy2DAsync(c->bounce[slot], width, (const char *)src + r0 * spitch, spitch, width,
+                            nr, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(c->bounce_ev[slot], s);
+    return e;
+  };
+  for (size_t i = 0; i < nchunks && i < 2; ++i) B2_CUDA_TRY(issue(i));
+  for (size_t i = 0; i < nchunks; ++i) {
+    const int slot = (int)(i & 1);
+    B2_CUDA_TRY(cudaEventSynchronize(c->bounce_ev[slot]));
+    const size_t r0 = i * per, nr = rows - r0 < per ? rows - r0 : per;
+    parallel_copy2d((char *)dst + r0 * dpitch, dpitch, c->bounce[slot], width, width, nr);
+    if (i + 2 < nchunks) B2_CUDA_TRY(issue(i + 2));
+  }
+  return B2_OK;
+}
+
 int stage_in(Ctx *c, int slot, const void *host, int rows, int cols, int ld, size_t elem,
              void **dev, int *dld, cudaStream_t s) {
   const int ldd = (rows + 1) & ~1;  // even leading dimension keeps 16-B vector loads legal
   void *d = workspace(c, slot, (size_t)(ldd > 0 ? ldd : 2) * (cols > 0 ? cols : 1) * elem);
   if (!d) return B2_ERR_NOMEM;
-  if (rows > 0 && cols > 0)
-    B2_CUDA_TRY(cudaMemcpy2DAsync(d, (size_t)ldd * elem, host, (size_t)ld * elem, (size_t)rows * elem,
-                                  cols, cudaMemcpyDefault, s));
   *dev = d;
   *dld = ldd > 0 ? ldd : 2;
+  if (rows > 0 && cols > 0)
+    return copy_h2d(c, d, (size_t)ldd * elem, host, (size_t)ld * elem, (size_t)rows * elem,
+                    (size_t)cols, s);
   return B2_OK;
 }
 
 int stage_out(void *host, int ld, const void *dev, int dld, int rows, int cols, size_t elem,
               cudaStream_t s) {
-  if (rows > 0 && cols > 0)
-    B2_CUDA_TRY(cudaMemcpy2DAsync(host, (size_t)ld * elem, dev, (size_t)dld * elem, (size_t)rows * elem,
-                                  cols, cudaMemcpyDefault, s));
-  return B2_OK;
+  if (rows <= 0 || cols <= 0) return B2_OK;
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  return copy_d2h(c, host, (size_t)ld * elem, dev, (size_t)dld * elem, (size_t)rows * elem,
+                  (size_t)cols, s);
 }
 
 static bool notrans(char c) { return c == 'N' || c == 'n'; }
@@ -452,14 +632,30 @@ static int gemm_dropin(char ta, char tb, int m, int n, int k, T alpha, const T *
     void *da = nullptr, *db = nullptr, *dc = nullptr;
     int dla = 2, dlb = 2, dlc = 2;
     int cw = n;
-    const int nb = need_ab ? pipeline_blocks(m, n, k, sizeof(T), &cw) : 1;
+    // Pageable operands go through the bounce buffers in one block (their
+    // host-side copies keep the host busy, so the column-block pipeline,
+    // which queues every copy up front, does not apply to them).
+    const bool pageable = host_pageable(cm) || (need_ab && (host_pageable(a) || host_pageable(b)));
+    const int nb = need_ab && !pageable ? pipeline_blocks(m, n, k, sizeof(T), &cw) : 1;
     st = B2_OK;
     if (nb == 1) {
       if (need_ab) {
         st = stage_in(c, WS_STAGE_A, a, ra, ca, lda, sizeof(T), &da, &dla, s);
         if (st == B2_OK) st = stage_in(c, WS_STAGE_B, b, rb, cb, ldb, sizeof(T), &db, &dlb, s);
       }
-      if (st == B2_OK) st = stage_in(c, WS_STAGE_C, cm, m, n, ldc, sizeof(T), &dc, &dlc, s);
+      // beta == 0 reads C only to keep a NaN or Inf already there: an
+      // all-finite host C is zeroed on the device instead of copied in
+      if (st == B2_OK && beta == (T)0 && need_ab && host_all_finite(cm, m, n, ldc)) {
+        dlc = (m + 1) & ~1;
+        dc = workspace(c, WS_STAGE_C, (size_t)dlc * n * sizeof(T));
+        if (!dc) st = B2_ERR_NOMEM;
+        else {
+          cudaError_t e = cudaMemsetAsync(dc, 0, (size_t)dlc * n * sizeof(T), s);
+          if (e != cudaSuccess) st = cuda_fail(e, "zero C");
+        }
+      } else if (st == B2_OK) {
+        st = stage_in(c, WS_STAGE_C, cm, m, n, ldc, sizeof(T), &dc, &dlc, s);
+      }
       if (st == B2_OK) st = run((const T *)da, dla, (const T *)db, dlb, (T *)dc, dlc, m, n, s);
       if (st == B2_OK) st = stage_out(cm, ldc, dc, dlc, m, n, sizeof(T), s);
     } else {

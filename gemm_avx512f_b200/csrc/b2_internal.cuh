@@ -63,6 +63,12 @@ struct Ctx {
   // Overlapped Ozaki schedule (created at its first use): the INT8 GEMMs run
   // on a high-priority stream while the slicing and reconstruction of other
   // column blocks run beside them on an auxiliary stream.
+  // Pinned bounce buffers for pageable (malloc'ed) host operands, created at
+  // their first use: host threads copy through them while the DMA of the
+  // other one runs.
+  static constexpr size_t BOUNCE_BYTES = 64ull << 20;
+  void *bounce[2] = {nullptr, nullptr};
+  cudaEvent_t bounce_ev[2] = {nullptr, nullptr};
   static constexpr int OZ_EVENTS = 2 * 16 + 3;  // per block: sliced, multiplied; fork, 2 joins
   cudaStream_t oz_gemm = nullptr, oz_aux = nullptr;
   cudaEvent_t oz_ev[OZ_EVENTS] = {};

@@ -58,6 +58,19 @@ int sgemm_dispatch(char ta, char tb, int m, int n, int k, float alpha, const flo
 int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                  const float *B, int ldb, float beta, float *C, int ldc, int method,
                  cudaStream_t s);
+// Engine configuration of a tensor-core SGEMM (sgemm_tc.cu): engine 0 =
+// single CTA 128 x 256 / 4 stages, 1 = single CTA 128 x 128 / 6 stages, 2 =
+// CTA pair 256 x 256 / 6 stages; split = K ranges (0 = automatic).
+struct SgCfg {
+  int engine = 0;
+  int split = 0;
+};
+SgCfg sgemm_default_cfg(int m, int n, int k, int method);
+// The selector's pick for a tensor-core SGEMM (tuner.cu; default without weights).
+SgCfg sgemm_pick_cfg(char ta, char tb, int m, int n, int k, int beta0, int method);
+int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                     const float *B, int ldb, float beta, float *C, int ldc, int method,
+                     const SgCfg &cfg, cudaStream_t s);
 int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                const float *B, int ldb, float beta, float *C, int ldc, cudaStream_t s);
 

@@ -247,9 +247,28 @@ int run_split(const float *Xp, long long sr, long long sk, int R, int K, int kp,
 
 }  // namespace
 
+// Tensor-core engine of an SGEMM call: 0 = single CTA, 128 x 256 tile, 4
+// stages; 1 = single CTA, 128 x 128 tile, 6 stages; 2 = CTA pair, 256 x 256
+// tile, 6 stages.  split: K ranges (0 = chosen from the tile count).
+int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                     const float *B, int ldb, float beta, float *C, int ldc, int method,
+                     const SgCfg &cfg, cudaStream_t s);
+
+SgCfg sgemm_default_cfg(int m, int n, int k, int method) {
+  (void)m, (void)n, (void)k, (void)method;
+  return SgCfg{0, 0};
+}
+
 int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                  const float *B, int ldb, float beta, float *C, int ldc, int method,
                  cudaStream_t s) {
+  return sgemm_tensor_cfg(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, method,
+                          sgemm_pick_cfg(ta, tb, m, n, k, beta == 0.f, method), s);
+}
+
+int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
+                     const float *B, int ldb, float beta, float *C, int ldc, int method,
+                     const SgCfg &cfg, cudaStream_t s) {
   if (m <= 0 || n <= 0) return B2_OK;
   Ctx *cx = ctx();
   if (!cx) return B2_ERR_NO_DEVICE;
@@ -282,30 +301,53 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
   }
   if (rc != B2_OK) return rc;
   const int kind = bf16 ? umma::KIND_BF16 : umma::KIND_TF32;
+  const int eng = (cfg.engine >= 0 && cfg.engine <= 2) ? cfg.engine : 0;
+  // tile: X rows (n side) per tile x Y rows (m side) per tile; TMA boxes per CTA
+  const int tile_p = eng == 2 ? 256 : umma::BM, tile_q = eng == 1 ? 128 : 256;
+  const int ybox = eng == 0 ? 256 : 128;
   CUtensorMap tmX, tmY;
   rc = umma::make_kmajor_map(&tmX, kind, Xp, ks_, n, 1, ks_ * esz, (long long)n * ks_ * esz,
                              umma::BM);
   if (rc == B2_OK)
-    rc = umma::make_kmajor_map(&tmY, kind, Yp, ks_, m, 1, ks_ * esz, (long long)m * ks_ * esz, 256);
+    rc = umma::make_kmajor_map(&tmY, kind, Yp, ks_, m, 1, ks_ * esz, (long long)m * ks_ * esz, ybox);
   if (rc != B2_OK) return rc;
   const int seg_kb = terms == 3 ? (int)((long long)kp * esz / umma::KBLOCK_BYTES) : 0;
-  const long long tiles = ((n + umma::BM - 1) / umma::BM) * (long long)((m + 255) / 256);
+  const long long tiles = ((n + tile_p - 1) / tile_p) * (long long)((m + tile_q - 1) / tile_q);
   const int kblocks = (int)((kt * esz + umma::KBLOCK_BYTES - 1) / umma::KBLOCK_BYTES);
-  int S = choose_ksplit(tiles, kblocks, cx->sm_count);
+  const int slots = eng == 2 ? cx->sm_count / 2 : cx->sm_count;
+  int S = cfg.split > 0 ? cfg.split : choose_ksplit(tiles, kblocks, slots);
+  if (S > kblocks) S = kblocks > 0 ? kblocks : 1;
   if (S > 1) {
     // the engine may merge ranges; size W for S and pass the count it uses
     const int kbps = (kblocks + S - 1) / S;
     S = (kblocks + kbps - 1) / kbps;
   }
+  auto run = [&](auto &&epi) -> int {
+    const char *nm = bf16 ? "sgemm_umma_bf16" : "sgemm_umma_tf32";
+    if (eng == 2)
+      return bf16 ? umma::launch_pair<umma::KIND_BF16, 256, 6>(tmX, tmY, n, m, kt, 1, epi,
+                                                               cx->device, cx->derr, s, nm,
+                                                               nullptr, S, seg_kb, segX, segY)
+                  : umma::launch_pair<umma::KIND_TF32, 256, 6>(tmX, tmY, n, m, kt, 1, epi,
+                                                               cx->device, cx->derr, s, nm,
+                                                               nullptr, S, seg_kb, segX, segY);
+    if (eng == 1)
+      return bf16 ? umma::launch<umma::KIND_BF16, 128, 6>(tmX, tmY, n, m, kt, 1, epi,
+                                                          cx->sm_count, cx->derr, s, nm, 0,
+                                                          nullptr, S, seg_kb, segX, segY)
+                  : umma::launch<umma::KIND_TF32, 128, 6>(tmX, tmY, n, m, kt, 1, epi,
+                                                          cx->sm_count, cx->derr, s, nm, 0,
+                                                          nullptr, S, seg_kb, segX, segY);
+    return bf16 ? umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
+                                                        cx->derr, s, nm, 0, nullptr, S, seg_kb,
+                                                        segX, segY)
+                : umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
+                                                        cx->derr, s, nm, 0, nullptr, S, seg_kb,
+                                                        segX, segY);
+  };
   if (S == 1) {
     F32Epi epi{C, ldc, m, n, alpha, beta};
-    if (bf16)
-      return umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
-                                                    cx->derr, s, "sgemm_umma_bf16", 0, nullptr,
-                                                    1, seg_kb, segX, segY);
-    return umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, epi, cx->sm_count,
-                                                  cx->derr, s, "sgemm_umma_tf32", 0, nullptr, 1,
-                                                  seg_kb, segX, segY);
+    return run(epi);
   }
   // Split-K: S partial products of K ranges, then one fixed-order reduction.
   const int ldw = (int)round_up(m, 256);  // whole 256-column tiles stay in bounds
@@ -313,12 +355,7 @@ int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float
   float *W = (float *)workspace(cx, WS_MISC, (size_t)plane * S * sizeof(float));
   if (!W) return B2_ERR_NOMEM;
   F32PartialEpi pe{W, plane, ldw, m, n};
-  rc = bf16 ? umma::launch<umma::KIND_BF16, 256, 4>(tmX, tmY, n, m, kt, 1, pe, cx->sm_count,
-                                                     cx->derr, s, "sgemm_umma_bf16", 0, nullptr, S,
-                                                     seg_kb, segX, segY)
-            : umma::launch<umma::KIND_TF32, 256, 4>(tmX, tmY, n, m, kt, 1, pe, cx->sm_count,
-                                                     cx->derr, s, "sgemm_umma_tf32", 0, nullptr, S,
-                                                     seg_kb, segX, segY);
+  rc = run(pe);
   if (rc != B2_OK) return rc;
   dim3 grid((unsigned)((m + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
   B2_PROF("sgemm_splitk_reduce", s);

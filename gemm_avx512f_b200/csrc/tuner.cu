@@ -10,6 +10,11 @@
 //   config 36..47  INT8 Ozaki emulation: moduli {13, 14, 15, 16}
 //                  x INT8 engine shape {128x256/4 stages, 128x128/6, 128x128/4}
 //
+// SGEMM (dtype 1): 3 tensor-core methods x engine {128x256 single CTA,
+// 128x128 single CTA, 256x256 CTA pair} x split-K {1, 2, 4, 8} (slots
+// decoded by decode_scfg below); the selector chooses within the method the
+// caller asked for.
+//
 // b2_tune_sweep times every configuration of every shape (minimum of `reps`
 // CUDA-event timings of back-to-back batches, inputs resident), the
 // exhaustive autotuner whose timing
@@ -151,6 +156,54 @@ int select_dgemm_method(Ctx *c, char ta, char tb, int m, int n, int k, int *slic
   return t.method;
 }
 
+// ------------------------------------------------------------ SGEMM space --
+// Configurations of the tensor-core SGEMM methods (dtype 1 of the selector):
+// slot c -> method c / 16 (TF32, TF32X3, BF16X3) and, within the method,
+// engine (c % 16) / 4 (0: single CTA 128x256 / 4 stages, 1: single CTA
+// 128x128 / 6 stages, 2: CTA pair 256x256 / 6 stages) x split-K {1, 2, 4, 8};
+// slots 12..15 of each method are unused (never timed, never chosen).
+constexpr int SG_PER_METHOD = 16;
+struct SgTune {
+  int method;
+  SgCfg cfg;
+  bool valid;
+};
+SgTune decode_scfg(int idx) {
+  SgTune t{};
+  const int mi = idx / SG_PER_METHOD, loc = idx % SG_PER_METHOD;
+  t.method = mi == 0 ? B2_METHOD_TF32 : mi == 1 ? B2_METHOD_TF32X3 : B2_METHOD_BF16X3;
+  t.valid = loc < 12;
+  t.cfg.engine = loc / 4;
+  t.cfg.split = 1 << (loc % 4);
+  return t;
+}
+int method_block(int method) {
+  return method == B2_METHOD_TF32 ? 0 : method == B2_METHOD_TF32X3 ? 1
+         : method == B2_METHOD_BF16X3 ? 2 : -1;
+}
+
+// Engine configuration for a tensor-core SGEMM: the learned selector's pick
+// among the method's configurations when weights are installed and the
+// shape lies in the trained range (every dimension <= 2048), else the
+// library default.
+SgCfg sgemm_pick_cfg(char ta, char tb, int m, int n, int k, int beta0, int method) {
+  std::vector<float> w;
+  {
+    std::lock_guard<std::mutex> lk(g_sel_mu);
+    w = g_sel_w;
+  }
+  const int blk = method_block(method);
+  if (w.empty() || blk < 0 || m > 2048 || n > 2048 || k > 2048)
+    return sgemm_default_cfg(m, n, k, method);
+  float x[MLP_IN], y[MLP_OUT];
+  mlp_features(ta, tb, m, n, k, 1, beta0, x);
+  mlp_forward_host(w.data(), x, y);
+  int best = -1;
+  for (int c = blk * SG_PER_METHOD; c < (blk + 1) * SG_PER_METHOD; ++c)
+    if (decode_scfg(c).valid && (best < 0 || y[c] < y[best])) best = c;
+  return decode_scfg(best).cfg;
+}
+
 int dgemm_auto(char ta, char tb, int m, int n, int k, double alpha, const double *A, int lda,
                const double *B, int ldb, double beta, double *C, int ldc, int slices,
                cudaStream_t s) {
@@ -162,6 +215,16 @@ int dgemm_auto(char ta, char tb, int m, int n, int k, double alpha, const double
 }
 
 namespace {
+__global__ void fill_uniform_f32_kernel(float *x, long long n, unsigned long long seed) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    x[i] = (float)((double)(z >> 11) * 0x1p-52 - 1.0);  // U[-1, 1)
+  }
+}
 __global__ void fill_uniform_kernel(double *x, long long n, unsigned long long seed) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
@@ -265,6 +328,105 @@ int b2_tune_sweep(int nshapes, const int *shapes, int reps, float *out_ms) {
   cudaFree(B);
   cudaFree(C);
   return rc;
+}
+
+int b2_sgemm_config(char transa, char transb, int m, int n, int k, float alpha, const float *A,
+                    int lda, const float *B, int ldb, float beta, float *C, int ldc, int config,
+                    void *stream) {
+  int info = 0;
+  if (config < 0 || config >= NCFG || !decode_scfg(config).valid) return B2_ERR_ARG;
+  int st = check_gemm(transa, transb, m, n, k, lda, ldb, ldc, A, B, C, &info);
+  if (st != B2_OK) return st;
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  const SgTune t = decode_scfg(config);
+  return sgemm_tensor_cfg(transa, transb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, t.method,
+                          t.cfg, pick_stream(c, stream));
+}
+
+int b2_tune_sweep_sgemm(int nshapes, const int *shapes, int reps, float *out_ms) {
+  if (nshapes < 0 || (nshapes > 0 && (!shapes || !out_ms)) || reps < 1) return B2_ERR_ARG;
+  Ctx *c = ctx();
+  if (!c) return B2_ERR_NO_DEVICE;
+  long long ma = 1, mb = 1, mc = 1;
+  for (int i = 0; i < nshapes; ++i) {
+    const long long m = shapes[6 * i], n = shapes[6 * i + 1], k = shapes[6 * i + 2];
+    if (m < 1 || n < 1 || k < 1) return B2_ERR_ARG;
+    ma = ma > m * k ? ma : m * k;
+    mb = mb > k * n ? mb : k * n;
+    mc = mc > m * n ? mc : m * n;
+  }
+  float *A = nullptr, *B = nullptr, *C = nullptr;
+  cudaEvent_t e0, e1;
+  if (cudaMalloc(&A, ma * 4) != cudaSuccess || cudaMalloc(&B, mb * 4) != cudaSuccess ||
+      cudaMalloc(&C, mc * 4) != cudaSuccess) {
+    (void)cudaGetLastError();
+    cudaFree(A);
+    cudaFree(B);
+    cudaFree(C);
+    return B2_ERR_NOMEM;
+  }
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaStream_t s = c->stream;
+  fill_uniform_f32_kernel<<<1024, 256, 0, s>>>(A, ma, 1);
+  fill_uniform_f32_kernel<<<1024, 256, 0, s>>>(B, mb, 2);
+  fill_uniform_f32_kernel<<<1024, 256, 0, s>>>(C, mc, 3);
+  int rc = B2_OK;
+  for (int i = 0; i < nshapes && rc == B2_OK; ++i) {
+    const int m = shapes[6 * i], n = shapes[6 * i + 1], k = shapes[6 * i + 2];
+    const char ta = shapes[6 * i + 3] ? 'T' : 'N', tb = shapes[6 * i + 4] ? 'T' : 'N';
+    const float beta = shapes[6 * i + 5] ? 0.f : 1.f;
+    const int lda = ta == 'N' ? m : k, ldb = tb == 'N' ? k : n;
+    for (int cfg = 0; cfg < NCFG && rc == B2_OK; ++cfg) {
+      const SgTune t = decode_scfg(cfg);
+      if (!t.valid) {
+        out_ms[(long long)i * NCFG + cfg] = __builtin_nanf("");
+        continue;
+      }
+      auto call = [&]() {
+        return sgemm_tensor_cfg(ta, tb, m, n, k, 1.f, A, lda, B, ldb, beta, C, m, t.method, t.cfg,
+                                s);
+      };
+      // batch of back-to-back calls sized to ~100 us, as in b2_tune_sweep
+      float single = 0.f;
+      cudaEventRecord(e0, s);
+      rc = call();
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "sweep");
+      cudaEventElapsedTime(&single, e0, e1);
+      int batch = single > 0.f ? (int)(0.1f / single) : 32;
+      batch = batch < 1 ? 1 : (batch > 32 ? 32 : batch);
+      float best = 1e30f;
+      for (int r = 0; r < reps && rc == B2_OK; ++r) {
+        cudaEventRecord(e0, s);
+        for (int b = 0; b < batch && rc == B2_OK; ++b) rc = call();
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = cuda_fail(cudaGetLastError(), "sweep");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)batch;
+        if (ms < best) best = ms;
+      }
+      out_ms[(long long)i * NCFG + cfg] = best;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(C);
+  return rc;
+}
+
+int b2_sgemm_selector_choose(int method, char transa, char transb, int m, int n, int k,
+                             int beta_zero) {
+  const int blk = method_block(method);
+  if (blk < 0 || m < 1 || n < 1 || k < 1) return -1;
+  const SgCfg cfg = sgemm_pick_cfg(transa, transb, m, n, k, beta_zero, method);
+  return blk * SG_PER_METHOD + cfg.engine * 4 +
+         (cfg.split >= 8 ? 3 : cfg.split >= 4 ? 2 : cfg.split >= 2 ? 1 : 0);
 }
 
 int b2_selector_set(const float *weights) {

@@ -461,7 +461,8 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 // ------------------------------------------------- CTA-pair (cta_group::2) --
-// The same product on a cluster of two CTAs that execute one 256 x BN MMA
+// The same product (work units of tile x K range, the three-term segment map)
+// on a cluster of two CTAs that execute one 256 x BN MMA
 // together (tcgen05.mma.cta_group::2): CTA r of the pair stages X rows
 // [256 tp + 128 r, +128) and Y rows [BN tq + (BN/2) r, +BN/2) of every
 // K-block in its own shared memory, and the even ("leader") CTA issues the
@@ -598,6 +599,8 @@ __global__ void __launch_bounds__(THREADS, 1)
   const int pair = (int)cluster_id_x(), npairs = (int)cluster_count_x();
   const int nbatch = pr.nbatch_dev ? min(*pr.nbatch_dev, pr.nbatch) : pr.nbatch;
   const int total_tiles = pr.tiles_p * pr.tiles_q * nbatch;
+  // work units: (tile, K range) pairs, the K range innermost
+  const int total_units = total_tiles * pr.ksplit;
   const uint32_t peer_abort = map_rank(smem_u32((const void *)abort_flag), rank ^ 1u);
 
   if (threadIdx.x == 0) {
@@ -637,12 +640,14 @@ __global__ void __launch_bounds__(THREADS, 1)
       int stage = 0;
       uint32_t phase = 0;
       bool ok = true;
-      for (int t = pair; t < total_tiles && ok; t += npairs) {
+      for (int u = pair; u < total_units && ok; u += npairs) {
+        const int t = u / pr.ksplit, ks = u - t * pr.ksplit;
         int b, tp, tq;
         tile_coords(pr, t, b, tp, tq);
         const int xrow = tp * PAIR_BM + (int)rank * BM;
         const int yrow = tq * BN + (int)rank * (BN / 2);
-        for (int kb = 0; kb < pr.kblocks; ++kb) {
+        const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait_pair(empty_bar(stage), phase ^ 1u, abort_flag, peer_abort, pr.derr,
                               pr.wait_ns)) {
             ok = false;
@@ -652,9 +657,15 @@ __global__ void __launch_bounds__(THREADS, 1)
           const uint32_t sy = sx + L::X_BYTES;
           const uint32_t fb = map_rank(full_bar(stage), 0);
           if (leader) mbar_expect_tx(full_bar(stage), 2 * L::STAGE_BYTES);
+          int kx = kb * kcoord, ky = kx;
+          if (pr.seg_kb) {
+            const int kq = kb / 3, tt = kb - 3 * kq;
+            kx = ((int)((pr.seg_x >> tt) & 1u) * pr.seg_kb + kq) * kcoord;
+            ky = ((int)((pr.seg_y >> tt) & 1u) * pr.seg_kb + kq) * kcoord;
+          }
           if (!(leader && pr.withhold && issued == 0)) {
-            tma_load_3d_pair(sx, &tmX, fb, kb * kcoord, xrow, b);
-            tma_load_3d_pair(sy, &tmY, fb, kb * kcoord, yrow, b);
+            tma_load_3d_pair(sx, &tmX, fb, kx, xrow, b);
+            tma_load_3d_pair(sy, &tmY, fb, ky, yrow, b);
           }
           ++issued;
           if (++stage == STAGES) { stage = 0; phase ^= 1u; }
@@ -672,7 +683,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t phase = 0;
       int it = 0;
       bool ok = true;
-      for (int t = pair; t < total_tiles && ok; t += npairs, ++it) {
+      for (int u = pair; u < total_units && ok; u += npairs, ++it) {
+        const int ks = u % pr.ksplit;
+        const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
         const int acc = it & 1;
         const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
         if (!mbar_wait_pair(tempty_bar(acc), acc_phase ^ 1u, abort_flag, peer_abort, pr.derr,
@@ -682,7 +695,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         tc_fence_after();
         const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-        for (int kb = 0; kb < pr.kblocks; ++kb) {
+        for (int kb = kb0; kb < kb1; ++kb) {
           if (!mbar_wait_pair(full_bar(stage), phase, abort_flag, peer_abort, pr.derr,
                               pr.wait_ns)) {
             ok = false;
@@ -694,7 +707,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
           for (int kk = 0; kk < KBLOCK_BYTES / 32; ++kk) {
             tc_mma_pair<KIND>(d_tmem, sw128_desc(sx + kk * 32), sw128_desc(sy + kk * 32), idesc,
-                              (kb | kk) ? 1u : 0u);
+                              (kb != kb0 || kk) ? 1u : 0u);
           }
           tc_commit_pair(empty_bar(stage), (uint16_t)3);  // frees the stage in both CTAs
           if (++stage == STAGES) { stage = 0; phase ^= 1u; }
@@ -709,7 +722,8 @@ __global__ void __launch_bounds__(THREADS, 1)
     // ---------------------------------------------------------- epilogue
     const int quarter = warp & 3;
     int it = 0;
-    for (int t = pair; t < total_tiles; t += npairs, ++it) {
+    for (int u = pair; u < total_units; u += npairs, ++it) {
+      const int t = u / pr.ksplit, ks = u - t * pr.ksplit;
       int b, tp, tq;
       tile_coords(pr, t, b, tp, tq);
       const int acc = it & 1;
@@ -724,7 +738,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         uint32_t v[32];
         tmem_ld32(taddr + (uint32_t)(c * 32), v);
         tmem_ld_wait(v);
-        epi(b, p, tq * BN + c * 32, v);
+        epi(b * pr.ksplit + ks, p, tq * BN + c * 32, v);  // batch x K range
       }
       tc_fence_before();
       __syncwarp();
@@ -822,7 +836,8 @@ int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long lo
 template <int KIND, int BN, int STAGES, class Epi>
 int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
                 int nbatch, const Epi &epi, int device, int *derr, cudaStream_t s,
-                const char *prof_name, const int *nbatch_dev = nullptr) {
+                const char *prof_name, const int *nbatch_dev = nullptr, int ksplit = 1,
+                int seg_kb = 0, unsigned seg_x = 0, unsigned seg_y = 0) {
   using L = SmemLayout<BN / 2, STAGES>;
   Problem pr;
   pr.P = P;
@@ -830,16 +845,22 @@ int launch_pair(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, lo
   pr.kblocks = (int)((kelems * elem_bytes(KIND) + KBLOCK_BYTES - 1) / KBLOCK_BYTES);
   pr.nbatch = nbatch;
   pr.nbatch_dev = nbatch_dev;
-  pr.ksplit = 1;
-  pr.kb_per_split = pr.kblocks;
-  pr.seg_kb = 0;  // the pair engine reads K' linearly
-  pr.seg_x = pr.seg_y = 0;
+  pr.seg_kb = seg_kb;
+  pr.seg_x = seg_x;
+  pr.seg_y = seg_y;
+  // split-K exactly as in launch(): ranges of ceil(kblocks / ksplit) blocks,
+  // their count recomputed so that none is empty
+  if (ksplit < 1) ksplit = 1;
+  if (ksplit > pr.kblocks) ksplit = pr.kblocks > 0 ? pr.kblocks : 1;
+  pr.kb_per_split = (pr.kblocks + ksplit - 1) / ksplit;
+  pr.ksplit = pr.kb_per_split > 0 ? (pr.kblocks + pr.kb_per_split - 1) / pr.kb_per_split : 1;
+  if (pr.ksplit < 1) pr.ksplit = 1;
   pr.tiles_p = (P + PAIR_BM - 1) / PAIR_BM;
   pr.tiles_q = (Q + BN - 1) / BN;
   pr.group = 8;
   pr.derr = derr;
   launch_wait_settings(&pr.wait_ns, &pr.withhold);
-  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch;
+  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch * pr.ksplit;
   if (total <= 0) return B2_OK;
   auto kern = umma_gemm_pair_kernel<KIND, BN, STAGES, Epi>;
   cudaLaunchConfig_t cfg = {};

@@ -352,9 +352,28 @@ B2_API int b2_dgemm_config(char transa, char transb, int m, int n, int k, double
  * buffers. */
 B2_API int b2_tune_sweep(int nshapes, const int *shapes, int reps, float *out_ms);
 
+/* SGEMM configuration space of the tensor-core methods (the selector's dtype
+ * 1): config c = method c / 16 (0 = TF32, 1 = TF32X3, 2 = BF16X3) and, for
+ * c % 16 < 12, engine (c % 16) / 4 (0 = single CTA 128x256 / 4 stages,
+ * 1 = single CTA 128x128 / 6 stages, 2 = CTA pair 256x256 / 6 stages) x
+ * split-K 1 << (c % 4); c % 16 >= 12 is unused (B2_ERR_ARG).  Replaces the
+ * compile-time SGEMM block sizes of sgemm_tune.h:6-15. */
+B2_API int b2_sgemm_config(char transa, char transb, int m, int n, int k, float alpha,
+                           const float *A, int lda, const float *B, int ldb, float beta,
+                           float *C, int ldc, int config, void *stream);
+/* Exhaustive SGEMM sweep over those 48 slots (unused slots NaN); same shape
+ * layout and timing rule as b2_tune_sweep, FP32 inputs. */
+B2_API int b2_tune_sweep_sgemm(int nshapes, const int *shapes, int reps, float *out_ms);
+/* Configuration the tensor-core SGEMM method `method` runs for this shape
+ * (the selector's pick when weights are installed and every dimension is at
+ * most 2048, else the library default); -1 for a non-tensor method. */
+B2_API int b2_sgemm_selector_choose(int method, char transa, char transb, int m, int n, int k,
+                                    int beta_zero);
+
 /* Learned selector: a 7-64-64-48 ReLU MLP predicting log2(ms) per
  * configuration from (log2 M, log2 N, log2 K centred at 7 and scaled by 1/3,
- * transA, transB, dtype, beta == 0).  b2_mlp_param_count() floats, layout
+ * transA, transB, dtype (0 = FP64: the 48 DGEMM configurations, 1 = FP32:
+ * the 48 SGEMM slots above), beta == 0).  b2_mlp_param_count() floats, layout
  * W1[7][64] b1 W2[64][64] b2 W3[64][48] b3.  Training, gradients and batched
  * inference run in this library's own CUDA kernels. */
 B2_API int b2_mlp_param_count(void);

@@ -70,26 +70,46 @@ def test_dgemm_dropin_matches_8x8_reference_drivers(cuda, method):
         blas.set_dgemm_method("fp64", 0)
 
 
+def _pinned(x):
+    """A copy of the Fortran array x in page-locked host memory."""
+    import torch
+
+    t = torch.empty(x.size, dtype=torch.from_numpy(x[:1, :1].copy()).dtype).pin_memory()
+    y = t.numpy().reshape(x.shape, order="F")
+    y[...] = x
+    return y, t  # keep t alive with y
+
+
+@pytest.mark.parametrize("host", ["pinned", "pageable"])
 @pytest.mark.parametrize("method,plant_nan", [("fp64", True), ("ozaki", True), ("fp64", False),
                                               ("ozaki", False)])
-def test_dgemm_dropin_pipelined_host_operands(cuda, method, plant_nan):
-    """Host operands of a product >= 2^32 flops go through the column-block
-    copy/compute/copy pipeline; blocks of 256-multiples leave a ragged last
-    block here (n = 1800), and op(B) blocks are row blocks of B for 'T'.
-    beta == 0 with an all-finite C skips copying C in (the device blocks are
-    zeroed); a NaN in C makes the library copy it, and the NaN survives."""
+def test_dgemm_dropin_pipelined_host_operands(cuda, method, plant_nan, host):
+    """Pinned host operands of a product >= 2^32 flops go through the
+    column-block copy/compute/copy pipeline; blocks of 256-multiples leave a
+    ragged last block here (n = 1800), and op(B) blocks are row blocks of B
+    for 'T'.  Pageable (malloc'ed) operands go through the library's pinned
+    bounce buffers in one block instead.  beta == 0 with an all-finite C skips
+    copying C in (the device blocks are zeroed); a NaN in C makes the library
+    copy it, and the NaN survives."""
     m, n, k = 1000, 1800, 1300
     rng = np.random.default_rng(77)
     u = np.finfo(np.float64).eps / 2
     blas.set_dgemm_method(method, 0)
+    keep = []
     try:
         for ta, tb in [("N", "N"), ("T", "T")]:
             a, b, c, ar, br = _case(rng, np.float64, m, n, k, ta, tb)
+            if host == "pinned":
+                (a, ka), (b, kb) = _pinned(a), _pinned(b)
+                keep += [ka, kb]
             if plant_nan:
                 c[5, 1700] = np.nan  # beta == 0 still multiplies C: NaN survives, as in the reference
             ref = c.copy(order="F")
             O.gemm(ta, tb, m, n, k, 1.25, a[:ar], b[:br], 0.0, ref[:m])
             got = c.copy(order="F")
+            if host == "pinned":
+                got, kc = _pinned(got)
+                keep.append(kc)
             blas.dgemm(ta, tb, m, n, k, 1.25, a, a.shape[0], b, b.shape[0], 0.0, got,
                        got.shape[0])
             assert np.array_equal(got[m:], c[m:]), "padding rows of C were written"

@@ -156,3 +156,82 @@ def test_heldout_regret_within_5_percent():
     if os.path.exists(rep):
         with open(rep) as fh:
             assert json.load(fh)["heldout"] == len(hold)
+
+
+def test_sgemm_heldout_regret_within_5_percent_per_method():
+    """The network chooses the engine and split-K of the tensor-core SGEMM
+    methods too (dtype input 1): on the held-out SGEMM shapes of the committed
+    timing database its pick is within 5 % of the exhaustive best of the
+    method, for each method, and no worse than the library default."""
+    db = os.path.join(DATA, f"tune_db_{KEY}.npz")
+    wp = os.path.join(DATA, f"selector_{KEY}.f32")
+    if not (os.path.exists(db) and os.path.exists(wp)):
+        pytest.skip("no committed timing database / selector")
+    z = np.load(db)
+    if "shapes_s" not in z:
+        pytest.skip("timing database without SGEMM sweep")
+    shapes, ntr = z["shapes_s"], int(z["train_s"])
+    ms = np.exp2(z["log2ms_s"].astype(np.float64))
+    hold, ms_h = shapes[ntr:], ms[ntr:]
+    w = np.fromfile(wp, np.float32)
+    L = _lib.lib()
+    for b, code in enumerate((_lib.METHODS["tf32"], _lib.METHODS["tf32x3"],
+                              _lib.METHODS["bf16x3"])):
+        valid = np.zeros(48, bool)
+        valid[16 * b:16 * b + 12] = True
+        best = np.where(valid[None, :], ms_h, np.inf).min(1)
+
+        def picks():
+            return np.array([L.b2_sgemm_selector_choose(code, b"T" if s[3] else b"N",
+                                                        b"T" if s[4] else b"N", int(s[0]),
+                                                        int(s[1]), int(s[2]), int(s[5]))
+                             for s in hold])
+
+        L.b2_selector_set(w.ctypes.data)
+        try:
+            pick = picks()
+        finally:
+            L.b2_selector_set(None)
+        dflt = picks()
+        assert valid[pick].all()
+        r = ms_h[np.arange(len(hold)), pick] / best - 1
+        rd = ms_h[np.arange(len(hold)), dflt] / best - 1
+        assert r.mean() <= 0.05, (b, r.mean())
+        assert np.exp(np.log1p(r).mean()) - 1 <= 0.05, (b, r.mean())
+        assert r.mean() <= rd.mean(), (b, r.mean(), rd.mean())
+
+
+@pytest.mark.gpu
+def test_every_sgemm_configuration_matches_the_oracle(cuda):
+    """Every engine / split-K slot of every tensor-core method (the space the
+    selector chooses from) computes the product: parity with the oracle, for
+    shapes that give the CTA pair both full and ragged tiles and several K
+    ranges."""
+    import torch
+
+    from oracle import oracle as O
+    from tests._util import normalized
+
+    L = _lib.lib()
+    U = {0: 2.0 ** -11, 1: 2.0 ** -21, 2: 2.0 ** -16}
+    rng = np.random.default_rng(17)
+    for (m, n, k, ta, tb) in [(300, 520, 700, "N", "T"), (512, 256, 1536, "T", "N")]:
+        a = np.asfortranarray(rng.uniform(-1, 1, (m, k) if ta == "N" else (k, m)).astype(np.float32))
+        b = np.asfortranarray(rng.uniform(-1, 1, (k, n) if tb == "N" else (n, k)).astype(np.float32))
+        c = np.asfortranarray(rng.uniform(-1, 1, (m, n)).astype(np.float32))
+        ref = O.gemm(ta, tb, m, n, k, np.float32(1.25), a, b, np.float32(-0.5), c.copy(order="F"))
+        da, db = (torch.from_numpy(x.T.copy()).to(cuda) for x in (a, b))
+        for cfg in range(48):
+            if cfg % 16 >= 12:
+                assert L.b2_sgemm_config(ta.encode(), tb.encode(), m, n, k, 1.0, da.data_ptr(),
+                                         a.shape[0], db.data_ptr(), b.shape[0], 0.0,
+                                         da.data_ptr(), m, cfg, None) == _lib.B2_ERR_ARG
+                continue
+            dc = torch.from_numpy(c.T.copy()).to(cuda)
+            torch.cuda.synchronize()
+            assert L.b2_sgemm_config(ta.encode(), tb.encode(), m, n, k, 1.25, da.data_ptr(),
+                                     a.shape[0], db.data_ptr(), b.shape[0], -0.5, dc.data_ptr(),
+                                     m, cfg, None) == 0
+            torch.cuda.synchronize()
+            got = np.asfortranarray(dc.cpu().numpy().T)
+            assert normalized(got, ref, k, a, b, U[cfg // 16]) <= 8, (cfg, m, n, k, ta, tb)
