@@ -316,7 +316,13 @@ struct CopyPool {
     job = nullptr;
   }
 };
-CopyPool g_copy_pool;
+// Never destroyed: its detached workers wait on its condition variable until
+// the process ends, and destroying a condition variable that threads wait on
+// blocks the exit.
+CopyPool &copy_pool() {
+  static CopyPool *pool = new CopyPool;
+  return *pool;
+}
 
 // rows x width bytes from src (pitch spitch) to dst (pitch dpitch), split over
 // the pool when large.
@@ -334,7 +340,7 @@ void parallel_copy2d(void *dst, size_t dpitch, const void *src, size_t spitch, s
     return;
   }
   const std::function<void(int)> f = body;
-  g_copy_pool.run(tasks, f);
+  copy_pool().run(tasks, f);
 }
 
 int bounce_ready(Ctx *c) {

@@ -220,17 +220,29 @@ __global__ void __launch_bounds__(WM *WN * 32, 1)
     __syncthreads();
     if (!last_slice) return;
     __threadfence();
-    const bool one = (beta == 1.0);
-    for (int idx = tid; idx < BM * BN; idx += NT) {
-      const int m = m0 + idx % BM, n = n0 + idx / BM;
-      if (m >= M || n >= N) continue;
-      const double *pp = P + (size_t)n * ldp + m;
-      double sum = 0.0;
-      for (int z = 0; z < (int)gridDim.z; ++z) sum += __ldcg(pp + (size_t)z * ldp * N);
-      double *c = C + (size_t)n * ldc + m;
-      *c = one ? fma(alpha, sum, *c) : fma(alpha, sum, beta * *c);
+    // The tile's slices summed in slice order into the accumulators, each
+    // thread over its own fragments (its own slice re-read from L2 where it
+    // just wrote it), all of one slice's loads in flight together; then the C
+    // epilogue below.
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+    for (int z = 0; z < (int)gridDim.z; ++z) {
+      const double *Pq = P + (size_t)z * ldp * N;
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NTL; ++j)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const int m = m0 + wm0 + i * 16 + g + 8 * (v >> 1);
+            const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
+            if (m < M && n < N) acc[i][j][v] += __ldcg(Pq + (size_t)n * ldp + m);
+          }
     }
-    return;
   }
   const bool beta_one = (beta == 1.0);
 #pragma unroll

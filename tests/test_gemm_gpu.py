@@ -14,6 +14,7 @@ from tests._util import normalized
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 TOL = 8.0
 
 SHAPES = [(1, 1, 1), (7, 5, 3), (37, 53, 29), (129, 65, 385), (513, 129, 1031), (64, 64, 4096),
@@ -78,6 +79,32 @@ def _pinned(x):
     y = t.numpy().reshape(x.shape, order="F")
     y[...] = x
     return y, t  # keep t alive with y
+
+
+def test_process_exits_after_pageable_copies(cuda, tmp_path):
+    """Pageable operands of 8 MiB are copied into the bounce buffers by the
+    library's host copy threads; a process that used them must still exit
+    promptly (the threads outlive every static destructor)."""
+    import subprocess
+    import sys
+
+    script = tmp_path / "pageable_exit.py"
+    script.write_text(
+        "import sys, numpy as np\n"
+        f"sys.path.insert(0, {ROOT!r})\n"
+        "from gemm_avx512f_b200 import blas\n"
+        "rng = np.random.default_rng(5)\n"
+        "n = 1024\n"
+        "a = np.asfortranarray(rng.uniform(-1, 1, (n, n)))\n"
+        "b = np.asfortranarray(rng.uniform(-1, 1, (n, n)))\n"
+        "c = np.zeros((n, n), order='F')\n"
+        "blas.dgemm('N', 'N', n, n, n, 1.0, a, n, b, n, 0.0, c, n)\n"
+        "e = np.abs(c - a @ b).max()\n"
+        "print('MAXERR', e)\n"
+        "sys.exit(0 if e < 1e-10 else 1)\n")
+    r = subprocess.run([sys.executable, str(script)], capture_output=True, text=True,
+                       timeout=180, cwd=ROOT, env=dict(os.environ, B2_METHOD="fp64"))
+    assert r.returncode == 0, r.stdout + r.stderr
 
 
 @pytest.mark.parametrize("host", ["pinned", "pageable"])

@@ -82,9 +82,9 @@ def test_dgemm_drop_in_shards_with_env_devices(cuda, tmp_path):
         "sys.exit(0 if e <= 8.0 else 1)\n")
     env = dict(os.environ, B2_DEVICES="0,0", B2_METHOD="fp64")
     r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True,
-                       timeout=600, cwd=ROOT)
+                       timeout=240, cwd=ROOT)
     assert r.returncode == 0, r.stdout + r.stderr
     env["B2_DEVICES"] = "0,99"
     r = subprocess.run([sys.executable, str(script)], env=env, capture_output=True, text=True,
-                       timeout=600, cwd=ROOT)
+                       timeout=240, cwd=ROOT)
     assert r.returncode != 0 and "B2Error" in r.stderr, r.stdout + r.stderr
