@@ -134,6 +134,7 @@ def lib() -> C.CDLL:
     L.b2_launch_count.restype = C.c_longlong
     L.b2_profile_enable.argtypes = [i]
     L.b2_profile_report.argtypes = [C.c_char_p, i]
+    L.b2_profile_timeline.argtypes = [C.c_char_p, i]
     for nm in ("b2_dgemm", "b2_dgemm_multi", "b2_sgemm", "b2_dgemm_dd", "b2_dtrsm", "b2_zgemm3m", "b2_cgemm3m",
                "b2_dgemm_error", "b2_device_error", "b2_set_dgemm_method", "b2_set_sgemm_method"):
         getattr(L, nm).restype = i
@@ -153,6 +154,18 @@ def profile_report() -> dict[str, tuple[int, float]]:
     for line in buf.value.decode().splitlines():
         name, cnt, ms = line.split()
         out[name] = (int(cnt), float(ms))
+    return out
+
+
+def profile_timeline() -> list[tuple[str, float, float]]:
+    """[(kernel name, start ms, end ms)] per launch since the last report, in
+    issue order, relative to the first launch's start (synchronizes)."""
+    buf = C.create_string_buffer(1 << 20)
+    lib().b2_profile_timeline(buf, len(buf))
+    out = []
+    for line in buf.value.decode().splitlines():
+        name, a, b = line.split()
+        out.append((name, float(a), float(b)))
     return out
 
 

@@ -1095,10 +1095,14 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   // on a high-priority stream while the slicing of later blocks and the
   // reconstruction of earlier ones (HBM- and FP64-bound) run beside it on an
   // auxiliary stream, so most of the auxiliary passes hide under the GEMMs.
-  const int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
-                 (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
-                    ? (n / 1024 < 2 ? 2 : (n / 1024 > 8 ? 8 : n / 1024))
-                    : 1;
+  // B2_OZAKI_BLOCKS = J (1 = no overlap, up to 16) fixes the block count.
+  const char *jenv = getenv("B2_OZAKI_BLOCKS");
+  const int jfix = jenv ? atoi(jenv) : 0;
+  int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
+           (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
+              ? (n / 1024 < 2 ? 2 : (n / 1024 > 8 ? 8 : n / 1024))
+              : 1;
+  if (J > 1 && jfix >= 1) J = jfix > 16 ? 16 : jfix;
   if (J > 1) {
     const int nb = (int)round_up((n + J - 1) / J, 256);
     const int nblk = (n + nb - 1) / nb;

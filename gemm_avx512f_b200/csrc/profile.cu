@@ -93,4 +93,30 @@ int b2_profile_report(char *buf, int len) {
   return (int)agg.size();
 }
 
+int b2_profile_timeline(char *buf, int len) {
+  int n = 0, off = 0;
+  if (buf && len > 0) buf[0] = 0;
+  cudaEvent_t t0 = g_prof.recs.empty() ? nullptr : g_prof.recs.front().a;
+  for (auto &r : g_prof.recs) {
+    float a = 0.f, b = 0.f;
+    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&a, t0, r.a) == cudaSuccess &&
+        cudaEventElapsedTime(&b, t0, r.b) == cudaSuccess) {
+      if (buf && len > 0 && off < len) {
+        int w = snprintf(buf + off, (size_t)(len - off), "%s %.6f %.6f\n", r.name, a, b);
+        if (w > 0 && off + w < len) off += w;
+        else off = len;
+      }
+      ++n;
+    } else {
+      (void)cudaGetLastError();
+    }
+  }
+  for (auto &r : g_prof.recs) {
+    g_prof.pool.push_back(r.a);
+    g_prof.pool.push_back(r.b);
+  }
+  g_prof.recs.clear();
+  return n;
+}
+
 }  // extern "C"
