@@ -613,8 +613,8 @@ __device__ __forceinline__ double crt_value(const double (&Sl)[S <= 15 ? 3 : 4],
 // multiply-adds per residue).  Rows/columns flagged NONFINITE use a direct
 // FP64 dot product.  Launched for the two possible counts of a call; the one
 // that is not the device-chosen count returns at once.
-template <int S>
-__global__ void __launch_bounds__(256, S <= 15 ? 2 : 1)
+template <int S, int E = (S <= 15 ? 8 : 4), int MINB = (S <= 15 ? 2 : 1)>
+__global__ void __launch_bounds__(256, MINB)
     reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr,
                        const int *__restrict__ s_dev, int M, int N,
                        const int *__restrict__ sigA, const int *__restrict__ tauB, double alpha,
@@ -622,8 +622,8 @@ __global__ void __launch_bounds__(256, S <= 15 ? 2 : 1)
                        const double *__restrict__ A, long long asr, long long ask,
                        const double *__restrict__ B, long long bsk, long long bsc, int K) {
   constexpr int LIMBS = S <= 15 ? 3 : 4;
-  constexpr int E = LIMBS == 3 ? 8 : 4;  // rows per thread (the 4-limb form needs more registers)
-  constexpr int WPR = E / 4;             // 32-bit residue words per modulus
+  static_assert(E == 4 || E == 8, "rows per thread: 4 or 8");
+  constexpr int WPR = E / 4;  // 32-bit residue words per modulus
   if (*s_dev != S) return;
   const int m0 = (blockIdx.x * blockDim.x + threadIdx.x) * E;
   if (m0 >= M) return;
