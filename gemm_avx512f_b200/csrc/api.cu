@@ -218,17 +218,6 @@ void *workspace(Ctx *c, int slot, size_t bytes) {
   return p;
 }
 
-int *fixup_counters(Ctx *c, size_t count, cudaStream_t s) {
-  const size_t bytes = (count < 1024 ? 1024 : count) * sizeof(int);
-  const bool fresh = c->ws_bytes[WS_FIXUP] < bytes;
-  int *p = (int *)workspace(c, WS_FIXUP, bytes);
-  if (p && fresh && cudaMemsetAsync(p, 0, c->ws_bytes[WS_FIXUP], s) != cudaSuccess) {
-    (void)cudaGetLastError();
-    return nullptr;
-  }
-  return p;
-}
-
 cudaStream_t pick_stream(Ctx *c, void *user_stream) {
   return user_stream ? (cudaStream_t)user_stream : c->stream;
 }

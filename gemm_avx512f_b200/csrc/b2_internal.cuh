@@ -33,7 +33,6 @@ enum WsSlot {
   WS_SPLIT_X, WS_SPLIT_Y,                   // SGEMM split planes
   WS_TRSM, WS_TRSM_INV, WS_TRSM_TMP, WS_3M, WS_GROUP, WS_ERR, WS_MISC,
   WS_KABI_A, WS_KABI_B, WS_KABI_D,         // kernel-ABI unpacked panels / 3M product
-  WS_FIXUP,                                 // split-K arrival counters (kept at zero)
   WS_COUNT
 };
 
@@ -88,7 +87,6 @@ int take_device_error(Ctx *c, int st);
 void *workspace(Ctx *c, int slot, size_t bytes);  // nullptr on allocation failure
 // At least `count` per-tile arrival counters, all zero (zeroed on `s` whenever
 // the array is (re)allocated; the kernels that use them leave them at zero).
-int *fixup_counters(Ctx *c, size_t count, cudaStream_t s);
 cudaStream_t pick_stream(Ctx *c, void *user_stream);
 
 // ------------------------------------------------------------- kernels --

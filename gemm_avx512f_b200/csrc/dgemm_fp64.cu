@@ -16,8 +16,11 @@
 //  * alpha/beta are applied once in the epilogue (the reference folds alpha
 //    into packed B, src/gemm_copy.c:64, and pre-scales C, :131).
 //  * Optional split-K: each z-slice writes an FP64 partial into workspace and
-//    the tile's last slice to finish adds them in slice order (deterministic)
-//    and applies alpha/beta -- no separate reduction launch.
+//    a reduction kernel adds them in slice order (deterministic) and applies
+//    alpha/beta.  Measured on B200 against an in-kernel fixup (the tile's last
+//    slice to arrive adds the partials): the separate reduction is faster on
+//    every shape tried, 14 us against 66 us at 128x128x1024 with 8 slices and
+//    83 us against 118 us at 1024^3 with 4.
 #include "b2_internal.cuh"
 #include "b2_profile.cuh"
 
@@ -103,17 +106,14 @@ __device__ __forceinline__ void dmma(double (&c)[4], const double *a, const doub
 
 // A_KCONT = transA (op(A)(m,k) = A[m*lda+k]); B_KCONT = !transB (op(B)(k,n) = B[n*ldb+k]).
 // Output: when P != nullptr the raw product of this CTA's K range is written to
-// P + z*ldp*N (split-K partial) and the last of the tile's gridDim.z CTAs to
-// arrive (counted in cnt[tile], which it resets to zero for the next launch)
-// adds the partials in slice order, still in L2, and writes
-// C = alpha*sum + beta*C; otherwise C = alpha*acc + beta*C (beta==1: C += alpha*acc).
+// P + z*ldp*N (split-K partial); otherwise C = alpha*acc + beta*C (beta==1: C += alpha*acc).
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MMAK, bool A_KCONT,
           bool B_KCONT, int VEC>
 __global__ void __launch_bounds__(WM *WN * 32, 1)
     dgemm_dmma_kernel(int M, int N, int K, int kchunk, double alpha,
                       const double *__restrict__ A, int lda, const double *__restrict__ B,
                       int ldb, double beta, double *__restrict__ C, int ldc,
-                      double *__restrict__ P, int ldp, int *__restrict__ cnt) {
+                      double *__restrict__ P, int ldp) {
   constexpr int NT = WM * WN * 32;
   constexpr int TM = BM / WM, TN = BN / WN;  // warp tile
   constexpr int MT = TM / 16, NTL = TN / 8;
@@ -206,43 +206,7 @@ __global__ void __launch_bounds__(WM *WN * 32, 1)
           const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
           if (m < M && n < N) Pz[(size_t)n * ldp + m] = acc[i][j][v];
         }
-    // In-kernel fixup: every slice publishes its partial (fence, then one
-    // arrival); the last to arrive sums all slices of the tile in order.
-    __shared__ int last_slice;
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-      const int tile = blockIdx.y * gridDim.x + blockIdx.x;
-      const int prev = atomicAdd(cnt + tile, 1);
-      last_slice = prev == (int)gridDim.z - 1;
-      if (last_slice) cnt[tile] = 0;  // every slice has arrived: ready for the next launch
-    }
-    __syncthreads();
-    if (!last_slice) return;
-    __threadfence();
-    // The tile's slices summed in slice order into the accumulators, each
-    // thread over its own fragments (its own slice re-read from L2 where it
-    // just wrote it), all of one slice's loads in flight together; then the C
-    // epilogue below.
-#pragma unroll
-    for (int i = 0; i < MT; ++i)
-#pragma unroll
-      for (int j = 0; j < NTL; ++j)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
-    for (int z = 0; z < (int)gridDim.z; ++z) {
-      const double *Pq = P + (size_t)z * ldp * N;
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NTL; ++j)
-#pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            const int m = m0 + wm0 + i * 16 + g + 8 * (v >> 1);
-            const int n = n0 + wn0 + j * 8 + 2 * t + (v & 1);
-            if (m < M && n < N) acc[i][j][v] += __ldcg(Pq + (size_t)n * ldp + m);
-          }
-    }
+    return;
   }
   const bool beta_one = (beta == 1.0);
 #pragma unroll
@@ -259,6 +223,20 @@ __global__ void __launch_bounds__(WM *WN * 32, 1)
           *p = beta_one ? fma(alpha, acc[i][j][v], c_old) : fma(alpha, acc[i][j][v], beta * c_old);
         }
       }
+}
+
+__global__ void splitk_reduce_kernel(int M, int N, int splits, const double *__restrict__ P,
+                                     int ldp, double alpha, double beta, double *__restrict__ C,
+                                     int ldc) {
+  const size_t total = (size_t)M * N;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int m = (int)(idx % M), n = (int)(idx / M);
+    double s = 0.0;
+    for (int z = 0; z < splits; ++z) s += P[(size_t)z * ldp * N + (size_t)n * ldp + m];
+    double *p = C + (size_t)n * ldc + m;
+    *p = (beta == 1.0) ? fma(alpha, s, *p) : fma(alpha, s, beta * *p);
+  }
 }
 
 template <typename T>
@@ -284,7 +262,6 @@ struct LaunchArgs {
   double *P;
   int ldp;
   int splits;
-  int *cnt;  // per-tile arrival counters of the split-K fixup (zero between launches)
 };
 
 template <int BM, int BN, int BK, int WM, int WN, int STAGES, int MMAK, bool AK, bool BKc,
@@ -300,7 +277,7 @@ cudaError_t launch_one(const LaunchArgs &a, cudaStream_t s) {
   dim3 grid((a.M + BM - 1) / BM, (a.N + BN - 1) / BN, a.splits);
   B2_PROF("dgemm_dmma", s);
   kern<<<grid, WM * WN * 32, SMEM, s>>>(a.M, a.N, a.K, a.kchunk, a.alpha, a.A, a.lda, a.B, a.ldb,
-                                        a.beta, a.C, a.ldc, a.P, a.ldp, a.cnt);
+                                        a.beta, a.C, a.ldc, a.P, a.ldp);
   return cudaGetLastError();
 }
 
@@ -326,25 +303,23 @@ inline bool is_notrans(char c) { return c == 'N' || c == 'n'; }
 }  // namespace
 
 Fp64Cfg fp64_default_cfg(int m, int n, int k, int sm_count) {
-  // The 64x64 tile (two CTAs per SM) is best from 1024^3 to 8192^3 on B200
-  // (31.5 TFLOPS at 4096^3).  Split-K only pays where it fills the machine
-  // better: the slice count S is the smallest that raises the fraction of
-  // busy CTA slots (work units / (waves x slots)) by more than 5 %, with
-  // every slice keeping >= 64 of K.  1024^3 (256 tiles, 86 % of one wave)
-  // therefore runs unsplit, 23.8 TFLOPS against 18.3 with 4 slices.
+  // Measured on B200: the 64x64 tile with two CTAs per SM is best from 1024^3
+  // to 8192^3 (31.5 TF at 4096^3); in the exhaustive sweep over 22000 shapes
+  // with M, N, K in [16, 1024] split-K 8 on that tile was the best single
+  // choice, so grids below ~1024 tiles split K up to 8 ways as long as every
+  // slice keeps >= 32 of K.  The split also stops at 1024 work units (tiles x
+  // slices): from 128 tiles on, 4 slices beat 8 on most shapes of that sweep,
+  // and 1024^3 runs in 83 us with 4 (25.9 TFLOPS) against 87 us unsplit and
+  // 90 us with 8; the partials' extra reduction traffic outweighs the finer
+  // wave fit.
+  (void)sm_count;
   Fp64Cfg c;
   c.tile = 2;
   c.mmak = 8;
-  const long long t64 = (long long)((m + 63) / 64) * ((n + 63) / 64);
-  const long long slots = 2LL * (sm_count > 0 ? sm_count : 148);
-  auto eff = [&](int s) {
-    const long long u = t64 * s, waves = (u + slots - 1) / slots;
-    return (double)u / (double)(waves * slots);
-  };
+  const long t64 = (long)((m + 63) / 64) * ((n + 63) / 64);
   int sk = 1;
-  double best = eff(1);
-  for (int s = 2; s <= 8 && k / s >= 64; s *= 2)
-    if (eff(s) > best + 0.05) best = eff(s), sk = s;
+  if (t64 < 1024)
+    while (sk < 8 && k / (2 * sk) >= 32 && t64 * sk * 2 <= 1024) sk *= 2;
   c.split_k = sk;
   return c;
 }
@@ -388,7 +363,7 @@ int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double
   const bool bk = is_notrans(tb);   // plain B: k contiguous
   const bool vec2 = (lda % 2 == 0) && (ldb % 2 == 0) && (((uintptr_t)A & 15) == 0) &&
                     (((uintptr_t)B & 15) == 0);
-  LaunchArgs a{m, n, k, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0, 1, nullptr};
+  LaunchArgs a{m, n, k, k, alpha, A, lda, B, ldb, beta, C, ldc, nullptr, 0, 1};
   int splits = cfg.split_k < 1 ? 1 : cfg.split_k;
   if (splits > 1) {
     int chunk = (k + splits - 1) / splits;
@@ -400,13 +375,8 @@ int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double
       const size_t bytes = (size_t)splits * m * n * sizeof(double);
       double *P = (double *)workspace(cx, WS_MISC, bytes);
       if (!P) return B2_ERR_NOMEM;
-      // arrival counters, one per tile of the finest (64 x 64) tiling
-      const size_t tiles = (size_t)((m + 63) / 64) * ((n + 63) / 64);
-      int *cnt = fixup_counters(cx, tiles, s);
-      if (!cnt) return B2_ERR_NOMEM;
       a.P = P;
       a.ldp = m;
-      a.cnt = cnt;
     } else {
       a.kchunk = k;
     }
@@ -423,6 +393,13 @@ int dgemm_fp64(char ta, char tb, int m, int n, int k, double alpha, const double
                   : launch_tile<4, 1>(cfg.tile, ak, bk, a, s);
   }
   if (e != cudaSuccess) return cuda_fail(e, "dgemm_dmma_kernel");
+  if (a.P) {
+    const size_t total = (size_t)m * n;
+    const int blocks = (int)((total + 255) / 256 > 4096 ? 4096 : (total + 255) / 256);
+    B2_PROF("dgemm_splitk_reduce", s);
+    splitk_reduce_kernel<<<blocks, 256, 0, s>>>(m, n, a.splits, a.P, a.ldp, alpha, beta, C, ldc);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
   return B2_OK;
 }
 
