@@ -606,14 +606,17 @@ __device__ __forceinline__ double crt_value(const double (&Sl)[S <= 15 ? 3 : 4],
 
 // C(m,n) = alpha * C'(m,n) 2^-(sigma_m + tau_n) + beta C(m,n) for a modulus
 // count S fixed at compile time (so every CRT weight is an immediate operand
-// from the constant bank).  Each thread handles E consecutive rows m (8, or 4
-// with 16 moduli) and walks the columns n with the grid's y stride; per column
+// from the constant bank).  Each thread handles E consecutive rows m and walks
+// the columns n with the grid's y stride; per column
 // it issues every load first -- S residue words and the C pairs -- then
 // accumulates the limb sums (one byte-to-double conversion and LIMBS fused
 // multiply-adds per residue).  Rows/columns flagged NONFINITE use a direct
 // FP64 dot product.  Launched for the two possible counts of a call; the one
 // that is not the device-chosen count returns at once.
-template <int S, int E = (S <= 15 ? 8 : 4), int MINB = (S <= 15 ? 2 : 1)>
+// Rows per thread E and resident blocks MINB: 4 and 4 up to 15 moduli (64
+// registers; 0.566 ms at 8192^2 x 15 moduli on B200 against 0.622 for 8 rows
+// and 2 blocks, same bits), 4 and 1 for 16 (the 4-limb form needs more).
+template <int S, int E = 4, int MINB = (S <= 15 ? 4 : 1)>
 __global__ void __launch_bounds__(256, MINB)
     reconstruct_kernel(const uint8_t *__restrict__ R, long long plane, int ldr,
                        const int *__restrict__ s_dev, int M, int N,
@@ -716,15 +719,15 @@ __global__ void __launch_bounds__(256, MINB)
   }
 }
 
-// Grid: x covers the row groups (8 rows per thread, 4 with 16 moduli; 256
-// threads per block); y strides over the columns.  ymax caps the y extent.
+// Grid: x covers the row groups (4 rows per thread, 256 threads per block);
+// y strides over the columns.  ymax caps the y extent.
 template <int S>
 void launch_reconstruct_s(unsigned ymax, cudaStream_t st, const uint8_t *R, long long plane,
                           int ldr, const int *s_dev, int M, int N, const int *sigA,
                           const int *tauB, double alpha, double beta, double *C, int ldc,
                           const double *A, long long asr, long long ask, const double *B,
                           long long bsk, long long bsc, int K) {
-  constexpr int E = S <= 15 ? 8 : 4;
+  constexpr int E = 4;
   const unsigned bx = (unsigned)(((M + E - 1) / E + 255) / 256);
   unsigned by = (unsigned)N < ymax ? (unsigned)N : ymax;
   if (by < 1u) by = 1u;
@@ -1098,9 +1101,13 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   // B2_OZAKI_BLOCKS = J (1 = no overlap, up to 16) fixes the block count.
   const char *jenv = getenv("B2_OZAKI_BLOCKS");
   const int jfix = jenv ? atoi(jenv) : 0;
+  // Blocks of about 4096 columns: measured at 8192^3 x 15 moduli on B200,
+  // 6.62 ms with 2 blocks, 6.71 with 4, 6.98 with 8 (the auxiliary passes
+  // gain little beside the persistent GEMM, which leaves them few registers
+  // and little shared memory, while each block boundary adds a GEMM tail).
   int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
            (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
-              ? (n / 1024 < 2 ? 2 : (n / 1024 > 8 ? 8 : n / 1024))
+              ? (n / 4096 < 2 ? 2 : (n / 4096 > 8 ? 8 : n / 4096))
               : 1;
   if (J > 1 && jfix >= 1) J = jfix > 16 ? 16 : jfix;
   if (J > 1) {
