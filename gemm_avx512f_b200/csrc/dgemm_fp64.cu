@@ -307,11 +307,12 @@ Fp64Cfg fp64_default_cfg(int m, int n, int k, int sm_count) {
   // to 8192^3 (31.5 TF at 4096^3); in the exhaustive sweep over 22000 shapes
   // with M, N, K in [16, 1024] split-K 8 on that tile was the best single
   // choice, so grids below ~1024 tiles split K up to 8 ways as long as every
-  // slice keeps >= 32 of K.  The split also stops at 1024 work units (tiles x
-  // slices): from 128 tiles on, 4 slices beat 8 on most shapes of that sweep,
-  // and 1024^3 runs in 83 us with 4 (25.9 TFLOPS) against 87 us unsplit and
-  // 90 us with 8; the partials' extra reduction traffic outweighs the finer
-  // wave fit.
+  // slice keeps >= 8 of K (2.6 % mean regret against the per-shape best of
+  // all 36 FP64 configurations; 32 % when slices had to keep >= 32: small-K
+  // products are latency-bound and gain from any split).  The split also
+  // stops at 1024 work units (tiles x slices): 1024^3 runs in 83 us with 4
+  // slices (25.9 TFLOPS) against 87 us unsplit and 90 us with 8; the
+  // partials' extra reduction traffic outweighs the finer wave fit.
   (void)sm_count;
   Fp64Cfg c;
   c.tile = 2;
@@ -319,7 +320,7 @@ Fp64Cfg fp64_default_cfg(int m, int n, int k, int sm_count) {
   const long t64 = (long)((m + 63) / 64) * ((n + 63) / 64);
   int sk = 1;
   if (t64 < 1024)
-    while (sk < 8 && k / (2 * sk) >= 32 && t64 * sk * 2 <= 1024) sk *= 2;
+    while (sk < 8 && k / (2 * sk) >= 8 && t64 * sk * 2 <= 1024) sk *= 2;
   c.split_k = sk;
   return c;
 }
