@@ -1,9 +1,10 @@
 // gemm3m.cu -- complex GEMM by the 3M method.
 //
-// zgemm3m runs in ONE fused launch at every size (zgemm3m_dmma_kernel, FP64
-// DMMA); cgemm3m runs in one fused FFMA launch below 2^24 multiply-adds and
-// otherwise as three 3xTF32 tensor-core GEMMs between a pre-add pass and a
-// combine pass (gemm3m_three_gemms, at the end).
+// zgemm3m runs in ONE fused launch (zgemm3m_dmma_kernel, FP64 DMMA) below 2^33
+// multiply-adds and as three FP64 DMMA GEMMs between a pre-add pass and a
+// combine pass above; cgemm3m runs in one fused FFMA launch below 2^24
+// multiply-adds and otherwise as three 3xTF32 tensor-core GEMMs
+// (gemm3m_three_gemms, at the end).
 //
 // Replaces the OpenBLAS gemm3m driver + the reference's 3M kernels
 // (zgemm3m_kernel_2x8_skylakex.c:336-351, zgemm3m_kernel_8x4_skylakex.c:309-334,
@@ -19,6 +20,8 @@
 // drivers (C scaled whenever beta != 1, src/gemm_driver.c:131).
 //   zgemm3m: FP64 DMMA (mma.sync.m16n8k4.f64), 64x64 tile, 8 warps of 32x16.
 //   cgemm3m: FP32 FFMA, 64x64 tile, 256 threads of 4x4 outputs.
+#include <stdlib.h>
+
 #include "b2_methods.cuh"
 #include "b2_profile.cuh"
 
@@ -528,10 +531,18 @@ int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T
     return B2_OK;
   }
   if constexpr (sizeof(T) == 8) {
-    // complex128: the one-launch DMMA kernel at every size (16-byte aligned
-    // operands, the normal case; an odd-aligned pointer takes the other paths)
+    // complex128: the one-launch DMMA kernel (16-byte aligned operands, the
+    // normal case; an odd-aligned pointer takes the other paths) below 2^33
+    // multiply-adds.  At 2048^3 the three DMMA GEMMs between a pre-add and a
+    // combine pass run at 38.0 TFLOPS effective against 36.4 for the one
+    // launch (tensor pipe 84 % against 75 % active: the 512-thread fused CTA
+    // holds one CTA per SM); B2_Z3M_FUSED_MAX (multiply-adds) moves the limit.
+    static const double fused_max = [] {
+      const char *e = getenv("B2_Z3M_FUSED_MAX");
+      return e ? atof(e) : 8589934592.0;
+    }();
     const bool al16 = (((uintptr_t)A | (uintptr_t)B | (uintptr_t)C) & 15) == 0;
-    if (al16) {
+    if (al16 && (double)m * n * k < fused_max) {
       const bool tA = !(ta == 'N' || ta == 'n' || ta == 'R' || ta == 'r');
       const bool tB = !(tb == 'N' || tb == 'n' || tb == 'R' || tb == 'r');
       const double sA = (ta == 'C' || ta == 'c' || ta == 'R' || ta == 'r') ? -1.0 : 1.0;

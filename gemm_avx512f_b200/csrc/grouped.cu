@@ -46,6 +46,29 @@ struct GroupDesc {
 // memory as As[k][m] and Bs[k][n] (stride GT_LD).  Tiles double-buffer the
 // panels: the next panel's loads are in flight while the current one is
 // multiplied.
+//
+// Element of a thread's e-th slot (idx = tid + 256 e, lane = idx % 32,
+// w = idx / 32): an operand whose m (or n) index is contiguous in memory
+// takes m = idx % 64, k = idx / 64 (one warp: 32 consecutive m of one k).  An
+// operand whose k is contiguous takes KL consecutive k per row (KL = 4
+// doubles or 8 floats, one 32-byte sector) over 32 / KL rows per warp:
+// k = lane % KL + KL (w % (16 / KL)), m = lane / KL + (32 / KL)(w / (16 / KL)).
+// Its shared-memory stores then hit every bank pair at most twice per warp
+// (stride 68: bank pair (8k + 2m) mod 32 for doubles, bank (4k + m) mod 32
+// for floats), where one k column of 16 k by 2 rows had hit each four times.
+template <typename T>
+__device__ __forceinline__ void panel_slot(int idx, bool kcont, int &mn, int &kk) {
+  if (!kcont) {
+    mn = idx % GT_M;
+    kk = idx / GT_M;
+    return;
+  }
+  constexpr int KL = 32 / (int)sizeof(T);  // 4 doubles or 8 floats: one 32-byte sector
+  const int lane = idx & 31, w = idx >> 5;
+  kk = lane % KL + KL * (w % (GT_K / KL));
+  mn = lane / KL + (32 / KL) * (w / (GT_K / KL));
+}
+
 template <typename T>
 struct PanelRegs {
   T a[4], b[4];
@@ -60,14 +83,14 @@ __device__ __forceinline__ void load_panel(const GroupDesc &g, int m0, int n0, i
   for (int e = 0; e < 4; ++e) {
     const int idx = threadIdx.x + 256 * e;
     int mm, kk;
-    if (g.ta) { kk = idx % GT_K; mm = idx / GT_K; } else { mm = idx % GT_M; kk = idx / GT_M; }
+    panel_slot<T>(idx, g.ta != 0, mm, kk);
     const int gm = m0 + mm, gk = k0 + kk;
     r.a[e] = (gm < g.m && gk < g.k)
                  ? (g.ta ? A[(long long)gm * g.lda + gk] : A[(long long)gk * g.lda + gm])
                  : (T)0;
-    int nn;
-    if (g.tb) { nn = idx % GT_N; kk = idx / GT_N; } else { kk = idx % GT_K; nn = idx / GT_K; }
-    const int gn = n0 + nn, gk2 = k0 + kk;
+    int nn, kb;
+    panel_slot<T>(idx, g.tb == 0, nn, kb);
+    const int gn = n0 + nn, gk2 = k0 + kb;
     r.b[e] = (gn < g.n && gk2 < g.k)
                  ? (g.tb ? B[(long long)gk2 * g.ldb + gn] : B[(long long)gn * g.ldb + gk2])
                  : (T)0;
@@ -81,11 +104,11 @@ __device__ __forceinline__ void store_panel(const GroupDesc &g, const PanelRegs<
   for (int e = 0; e < 4; ++e) {
     const int idx = threadIdx.x + 256 * e;
     int mm, kk;
-    if (g.ta) { kk = idx % GT_K; mm = idx / GT_K; } else { mm = idx % GT_M; kk = idx / GT_M; }
+    panel_slot<T>(idx, g.ta != 0, mm, kk);
     As[kk * GT_LD + mm] = r.a[e];
-    int nn;
-    if (g.tb) { nn = idx % GT_N; kk = idx / GT_N; } else { kk = idx % GT_K; nn = idx / GT_K; }
-    Bs[kk * GT_LD + nn] = r.b[e];
+    int nn, kb;
+    panel_slot<T>(idx, g.tb == 0, nn, kb);
+    Bs[kb * GT_LD + nn] = r.b[e];
   }
 }
 

@@ -18,15 +18,24 @@ namespace {
 // instruction, so the FFMA pipe, not instruction issue, is the limit).
 // CTA tile 128 x 128, K blocks of 16, 256 threads of 8 x 8 outputs, K panels
 // staged through registers (16-byte global loads when the layout allows)
-// into double-buffered shared memory.  A is stored in shared memory with every
-// value duplicated, (a, a), so one 16-byte shared load yields the two
-// broadcast pairs that multiply a pair of B values; thread (tx, ty) owns rows
-// 2 tx + {0, 1} + 32 q (q = 0..3: conflict-free 16-byte loads across the
-// half-warp) and columns 4 ty + {0..3} + 64 h (h = 0, 1).
+// into double-buffered shared memory.  Thread (tx, ty) owns rows
+// 4 tx + {0..3} + 64 h' and columns 4 ty + {0..3} + 64 h (h', h = 0, 1): per
+// K step it reads two 16-byte A vectors and two 16-byte B vectors (64 bytes
+// for 64 FMAs -- the shared-memory rate of 128 bytes per clock per SM then
+// matches the 128 FMAs per clock) and forms the broadcast pairs (a, a) in
+// registers.  Storing A duplicated in shared memory instead (one 16-byte load
+// giving two pairs) cost 96 bytes per 64 FMAs and made the kernel
+// shared-memory bound (ncu at 4096^3: L1 84 % busy, FMA pipe 55 %).
 constexpr int S2_M = 128, S2_N = 128, S2_K = 16, S2_APAD = 4, S2_BPAD = 4;
-constexpr int S2_ALD = 2 * S2_M + S2_APAD;  // floats per k row of the duplicated A panel
+constexpr int S2_ALD = S2_M + S2_APAD;  // floats per k row of the A panel
 constexpr int S2_BLD = S2_N + S2_BPAD;
 constexpr int S2_SMEM = (2 * S2_K * S2_ALD + 2 * S2_K * S2_BLD) * 4;
+
+__device__ __forceinline__ unsigned long long dup2(float a) {
+  unsigned long long d;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(d) : "f"(a));
+  return d;
+}
 
 __device__ __forceinline__ void ffma2(unsigned long long &c, unsigned long long a,
                                       unsigned long long b) {
@@ -52,12 +61,12 @@ __global__ void __launch_bounds__(256, 1)
                        const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
                        int ldc) {
   extern __shared__ __align__(16) float s2mem[];
-  float *As = s2mem;                        // [2][S2_K][S2_ALD] duplicated pairs
+  float *As = s2mem;                        // [2][S2_K][S2_ALD]
   float *Bs = s2mem + 2 * S2_K * S2_ALD;    // [2][S2_K][S2_BLD]
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int m0 = blockIdx.x * S2_M, n0 = blockIdx.y * S2_N;
 
-  unsigned long long acc[8][4];  // row r: 2tx + (r&1) + 32(r>>1); column pair c
+  unsigned long long acc[8][4];  // row r: 4tx + (r&3) + 64(r>>2); column pair c
 #pragma unroll
   for (int r = 0; r < 8; ++r)
 #pragma unroll
@@ -93,17 +102,14 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int c = tid + 256 * h;
-      const float av[4] = {ra[h].x, ra[h].y, ra[h].z, ra[h].w};
-      if (!TA) {  // two 16-byte stores of duplicated pairs
+      if (!TA) {
         const int kk = c >> 5, mm = (c & 31) * 4;
-        float *d = as + kk * S2_ALD + 2 * mm;
-        *reinterpret_cast<float4 *>(d) = make_float4(av[0], av[0], av[1], av[1]);
-        *reinterpret_cast<float4 *>(d + 4) = make_float4(av[2], av[2], av[3], av[3]);
+        *reinterpret_cast<float4 *>(as + kk * S2_ALD + mm) = ra[h];
       } else {
         const int mm = c >> 2, kk = (c & 3) * 4;
+        const float av[4] = {ra[h].x, ra[h].y, ra[h].z, ra[h].w};
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
-          *reinterpret_cast<float2 *>(as + (kk + e) * S2_ALD + 2 * mm) = make_float2(av[e], av[e]);
+        for (int e = 0; e < 4; ++e) as[(kk + e) * S2_ALD + mm] = av[e];
       }
       if (TB) {
         const int kk = c >> 5, nn = (c & 31) * 4;
@@ -128,22 +134,26 @@ __global__ void __launch_bounds__(256, 1)
     const float *bs = Bs + buf * S2_K * S2_BLD;
 #pragma unroll
     for (int kk = 0; kk < S2_K; ++kk) {
-      ulonglong2 a2[4];  // duplicated pairs of rows 32q + 2tx and 32q + 2tx + 1
+      float av[8];  // rows 4tx + i + 64h'
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        a2[q] = *reinterpret_cast<const ulonglong2 *>(as + kk * S2_ALD + 2 * (32 * q + 2 * tx));
+      for (int hh = 0; hh < 2; ++hh) {
+        const float4 v = *reinterpret_cast<const float4 *>(as + kk * S2_ALD + 64 * hh + 4 * tx);
+        av[4 * hh] = v.x;
+        av[4 * hh + 1] = v.y;
+        av[4 * hh + 2] = v.z;
+        av[4 * hh + 3] = v.w;
+      }
       ulonglong2 b2[2];  // columns 64h + 4ty .. 64h + 4ty + 3
 #pragma unroll
       for (int h = 0; h < 2; ++h)
         b2[h] = *reinterpret_cast<const ulonglong2 *>(bs + kk * S2_BLD + 64 * h + 4 * ty);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int r = 0; r < 8; ++r) {
+        const unsigned long long a = dup2(av[r]);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          ffma2(acc[2 * q][2 * h], a2[q].x, b2[h].x);
-          ffma2(acc[2 * q][2 * h + 1], a2[q].x, b2[h].y);
-          ffma2(acc[2 * q + 1][2 * h], a2[q].y, b2[h].x);
-          ffma2(acc[2 * q + 1][2 * h + 1], a2[q].y, b2[h].y);
+          ffma2(acc[r][2 * h], a, b2[h].x);
+          ffma2(acc[r][2 * h + 1], a, b2[h].y);
         }
       }
     }
@@ -157,7 +167,7 @@ __global__ void __launch_bounds__(256, 1)
   const bool beta_one = (beta == 1.f);
 #pragma unroll
   for (int r = 0; r < 8; ++r) {
-    const int m = m0 + 2 * tx + (r & 1) + 32 * (r >> 1);
+    const int m = m0 + 4 * tx + (r & 3) + 64 * (r >> 2);
     if (m >= M) continue;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {

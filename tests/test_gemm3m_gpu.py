@@ -93,3 +93,33 @@ def test_gemm3m_beta_semantics_and_device_api(cuda):
     blas.zgemm3m_device("N", "N", m, n, k, 1.0, da, m, db, k, 0.0, dc, m)
     torch.cuda.synchronize()
     np.testing.assert_allclose(dc.cpu().numpy().T, a @ b, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("C", "T")])
+def test_zgemm3m_three_gemm_path_large(cuda, ta, tb):
+    """From 2^33 multiply-adds zgemm3m runs three FP64 DMMA GEMMs between a
+    pre-add and a combine pass: 2048^3 against the complex128 product of
+    torch on the same device (plain FP64 reference of the same op)."""
+    import torch
+
+    n = 2048
+    g = torch.Generator(device=cuda).manual_seed(11)
+    A = torch.complex(torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1,
+                      torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
+    B = torch.complex(torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1,
+                      torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
+    C0 = torch.complex(torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g),
+                       torch.zeros(n, n, device=cuda, dtype=torch.float64))
+    # storage is column-major: the tensors hold the transposes of the matrices
+    Am, Bm = A.t(), B.t()
+    op = {"N": lambda x: x, "T": lambda x: x.t(), "C": lambda x: x.conj().t()}
+    al, be = 0.75 - 1.25j, 0.5 + 0.25j
+    ref = al * (op[ta](Am) @ op[tb](Bm)) + be * C0.t()
+    C = C0.clone()
+    blas.zgemm3m_device(ta, tb, n, n, n, al, A, n, B, n, be, C, n)
+    torch.cuda.synchronize()
+    got = C.t()
+    u = 2.0 ** -53
+    den = n * u * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B)) * abs(al)
+    err = float(torch.linalg.norm(got - ref)) / den
+    assert err <= 8, (ta, tb, err)

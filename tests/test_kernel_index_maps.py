@@ -4,7 +4,7 @@ element is loaded exactly once, and every shared-memory access stays inside
 its buffer.
 
 * the paired-FMA FP32 kernel (csrc/sgemm.cu, sgemm_ffma2_kernel): 128 x 128
-  tile, K blocks of 16, 256 threads, duplicated A panel;
+  tile, K blocks of 16, 256 threads, 8 x 8 outputs each;
 * the one-launch 3M kernel (csrc/gemm3m.cu, zgemm3m_dmma_kernel): 64 x 64
   complex tile, K blocks of 16, 16 warps of 16 x 16, DMMA m16n8k8 fragments.
 """
@@ -12,7 +12,7 @@ import itertools
 
 # ---------------------------------------------------------- sgemm_ffma2 ----
 S2_M, S2_N, S2_K = 128, 128, 16
-S2_ALD, S2_BLD = 2 * S2_M + 4, S2_N + 4
+S2_ALD, S2_BLD = S2_M + 4, S2_N + 4
 A_FLOATS, B_FLOATS = S2_K * S2_ALD, S2_K * S2_BLD  # one buffer each
 
 
@@ -21,7 +21,7 @@ def test_ffma2_outputs_owned_once():
     for tid in range(256):
         tx, ty = tid & 15, tid >> 4
         for r in range(8):
-            m = 2 * tx + (r & 1) + 32 * (r >> 1)
+            m = 4 * tx + (r & 3) + 64 * (r >> 2)
             for c in range(4):
                 nb = 64 * (c >> 1) + 4 * ty + 2 * (c & 1)
                 for e in range(2):
@@ -40,15 +40,19 @@ def test_ffma2_staging_covers_panels_once_and_stays_in_bounds():
                 if not ta:
                     kk, mm = c >> 5, (c & 31) * 4
                     elems = [(mm + e, kk) for e in range(4)]
-                    offs = [kk * S2_ALD + 2 * mm + j for j in range(8)]
+                    offs = [kk * S2_ALD + mm + e for e in range(4)]
+                    assert (kk * S2_ALD + mm) % 4 == 0  # 16-byte store
                 else:
                     mm, kk = c >> 2, (c & 3) * 4
                     elems = [(mm, kk + e) for e in range(4)]
-                    offs = [(kk + e) * S2_ALD + 2 * mm + j for e in range(4) for j in range(2)]
+                    offs = [(kk + e) * S2_ALD + mm for e in range(4)]
                 for x in elems:
                     assert x not in a_seen
                     a_seen.add(x)
                 assert all(0 <= o < A_FLOATS for o in offs)
+                # the stored element sits where the fragment load expects it
+                for (m_, k_), o in zip(elems, offs):
+                    assert o == k_ * S2_ALD + m_
                 if tb:
                     kk, nn = c >> 5, (c & 31) * 4
                     elems = [(kk, nn + e) for e in range(4)]
@@ -68,11 +72,12 @@ def test_ffma2_fragment_loads_in_bounds_and_match_owned_rows():
     for tid in range(256):
         tx, ty = tid & 15, tid >> 4
         for kk in range(S2_K):
-            for q in range(4):
-                base = kk * S2_ALD + 2 * (32 * q + 2 * tx)
+            for hh in range(2):
+                base = kk * S2_ALD + 64 * hh + 4 * tx
                 assert base % 4 == 0 and base + 3 < A_FLOATS  # 16-byte aligned load
-                # floats [0,1] = dup of row 32q + 2tx, [2,3] = dup of row 32q + 2tx + 1
-                assert (base - kk * S2_ALD) // 2 == 32 * q + 2 * tx
+                # floats [0..3] = rows 4tx + i + 64hh, the rows r = 4hh + i of the thread
+                for i in range(4):
+                    assert base + i - kk * S2_ALD == 4 * tx + ((4 * hh + i) & 3) + 64 * ((4 * hh + i) >> 2)
             for h in range(2):
                 base = kk * S2_BLD + 64 * h + 4 * ty
                 assert base % 4 == 0 and base + 3 < B_FLOATS
@@ -80,15 +85,13 @@ def test_ffma2_fragment_loads_in_bounds_and_match_owned_rows():
 
 def test_ffma2_quarter_warp_a_loads_conflict_free():
     # 16-byte loads run in quarter-warp phases: each phase's 8 threads must
-    # touch distinct 16-byte slots of a 128-byte window (lanes 16-31 repeat
-    # lanes 0-15's addresses, a broadcast)
+    # touch distinct 16-byte slots of a 128-byte window
     for kk in range(S2_K):
-        for q in range(4):
+        for hh in range(2):
             for quarter in range(4):
                 lanes = range(8 * quarter, 8 * quarter + 8)
-                slots = {((kk * S2_ALD + 2 * (32 * q + 2 * (l & 15))) * 4 // 16) % 8
-                         for l in lanes}
-                assert len(slots) == len({l & 15 for l in lanes})
+                slots = {((kk * S2_ALD + 64 * hh + 4 * (l & 15)) * 4 // 16) % 8 for l in lanes}
+                assert len(slots) == 8
 
 
 # ------------------------------------------------------ zgemm3m_dmma ----
@@ -153,3 +156,52 @@ def test_z_fragment_loads_conflict_free():
                 off = g * (Z_BK + 4) + t if kc else t * (Z_BM + 2) + g
                 slots.add((off * 16 // 16) % 8)
             assert len(slots) == 8, (kc, phase)
+
+
+# ------------------------------------------------------ grouped panels ----
+GT_M, GT_K, GT_LD = 64, 16, 68
+
+
+def panel_slot(idx, kcont, esz):
+    if not kcont:
+        return idx % GT_M, idx // GT_M
+    kl = 32 // esz
+    lane, w = idx & 31, idx >> 5
+    return lane // kl + (32 // kl) * (w // (GT_K // kl)), lane % kl + kl * (w % (GT_K // kl))
+
+
+def test_grouped_panel_slots_cover_the_panel_once():
+    for esz in (8, 4):
+        for kcont in (False, True):
+            seen = {panel_slot(tid + 256 * e, kcont, esz) for tid in range(256) for e in range(4)}
+            assert len(seen) == GT_M * GT_K
+            assert all(0 <= mn < GT_M and 0 <= k < GT_K for mn, k in seen)
+            assert all(k * GT_LD + mn < GT_K * GT_LD for mn, k in seen)
+
+
+def test_grouped_panel_stores_hit_each_bank_at_most_twice():
+    # per warp store: doubles occupy bank pairs (word offset 2 x element), floats one bank
+    for esz in (8, 4):
+        for kcont in (False, True):
+            for w in range(32):
+                hits = {}
+                for lane in range(32):
+                    mn, k = panel_slot(32 * w + lane, kcont, esz)
+                    bank = ((k * GT_LD + mn) * (esz // 4)) % 32
+                    hits[bank] = hits.get(bank, 0) + 1
+                # 32 lanes x 8 B need 2 wavefronts anyway; floats need 1 (allow 2)
+                assert max(hits.values()) <= 2, (esz, kcont, w, hits)
+
+
+def test_grouped_kcont_loads_use_whole_sectors():
+    # a k-contiguous warp load reads whole 32-byte sectors of each row
+    for esz in (8, 4):
+        for w in range(32):
+            rows = {}
+            for lane in range(32):
+                mn, k = panel_slot(32 * w + lane, True, esz)
+                rows.setdefault(mn, []).append(k)
+            for ks in rows.values():
+                ks.sort()
+                assert len(ks) * esz == 32 and ks == list(range(ks[0], ks[0] + len(ks)))
+                assert (ks[0] * esz) % 32 == 0
