@@ -229,27 +229,28 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
     }
 }
 
+// tile_prob[t] is the problem that owns flattened tile t (one load instead of
+// a binary search of dependent descriptor loads).  Thread 0 fetches the next
+// tile index while the current tile runs, so the counter's round trip is
+// hidden too.
 __global__ void __launch_bounds__(256, 3)
-    grouped_kernel(const GroupDesc *__restrict__ d, int count, long long total_tiles,
-                   unsigned long long *counter) {
+    grouped_kernel(const GroupDesc *__restrict__ d, const int *__restrict__ tile_prob,
+                   long long total_tiles, unsigned long long *counter) {
   __shared__ __align__(16) double sm[2 * GT_STAGE];  // two stages of A and B panels
-  __shared__ long long tile_s;
-  for (;;) {
-    __syncthreads();
-    if (threadIdx.x == 0) tile_s = (long long)atomicAdd(counter, 1ull);
-    __syncthreads();
-    const long long t = tile_s;
-    if (t >= total_tiles) break;
-    int lo = 0, hi = count - 1;  // last problem whose first tile <= t
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (d[mid].tile_offset <= t) lo = mid; else hi = mid - 1;
-    }
-    const GroupDesc g = d[lo];
+  __shared__ long long next_s;
+  if (threadIdx.x == 0) next_s = (long long)atomicAdd(counter, 1ull);
+  __syncthreads();
+  long long t = next_s;
+  while (t < total_tiles) {
+    __syncthreads();  // every thread has read next_s
+    if (threadIdx.x == 0) next_s = (long long)atomicAdd(counter, 1ull);
+    const GroupDesc g = d[tile_prob[t]];
     const int local = (int)(t - g.tile_offset);
     const int m0 = (local % g.tiles_m) * GT_M, n0 = (local / g.tiles_m) * GT_N;
     if (g.dtype == 0) tile_f64(g, m0, n0, sm);
     else tile_f32(g, m0, n0, reinterpret_cast<float *>(sm));
+    __syncthreads();  // thread 0's store of next_s is visible
+    t = next_s;
   }
 }
 
@@ -257,7 +258,9 @@ struct Plan {
   int device = -1;
   int count = 0;
   long long total_tiles = 0;
+  bool owns = true;  // device buffers allocated for this plan (else context workspace)
   GroupDesc *d_desc = nullptr;
+  int *d_map = nullptr;  // tile -> problem
   unsigned long long *d_counter = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -267,7 +270,7 @@ struct Plan {
 bool is_nt(char c) { return c == 'N' || c == 'n'; }
 
 int build_descs(int count, const b2_gemm_problem *pr, std::vector<GroupDesc> &out,
-                long long *total, int *info) {
+                std::vector<int> &map, long long *total, int *info) {
   std::vector<int> order(count);
   std::iota(order.begin(), order.end(), 0);
   // largest K first: each tile costs ~K, so the long tiles are dequeued first
@@ -303,7 +306,13 @@ int build_descs(int count, const b2_gemm_problem *pr, std::vector<GroupDesc> &ou
     g.tiles_n = (p.n + GT_N - 1) / GT_N;
     g.tile_offset = off;
     off += (long long)g.tiles_m * g.tiles_n;
+    if (off > (1ll << 31)) { *info = idx + 1; return B2_ERR_ARG; }
     out.push_back(g);
+  }
+  map.resize((size_t)off);
+  for (size_t i = 0; i < out.size(); ++i) {
+    const long long t1 = i + 1 < out.size() ? out[i + 1].tile_offset : off;
+    for (long long t = out[i].tile_offset; t < t1; ++t) map[(size_t)t] = (int)i;
   }
   *total = off;
   return B2_OK;
@@ -313,7 +322,7 @@ int enqueue(const Plan &p, cudaStream_t s) {
   B2_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned long long), s));
   if (p.total_tiles == 0) return B2_OK;
   B2_PROF("grouped_gemm", s);
-  grouped_kernel<<<p.grid, 256, 0, s>>>(p.d_desc, p.count, p.total_tiles, p.d_counter);
+  grouped_kernel<<<p.grid, 256, 0, s>>>(p.d_desc, p.d_map, p.total_tiles, p.d_counter);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -322,17 +331,24 @@ void free_plan(Plan *p) {
   if (!p) return;
   if (p->exec) cudaGraphExecDestroy(p->exec);
   if (p->graph) cudaGraphDestroy(p->graph);
-  if (p->d_desc) cudaFree(p->d_desc);
-  if (p->d_counter) cudaFree(p->d_counter);
+  if (p->owns) {
+    if (p->d_desc) cudaFree(p->d_desc);
+    if (p->d_map) cudaFree(p->d_map);
+    if (p->d_counter) cudaFree(p->d_counter);
+  }
   delete p;
 }
 
+// A plan for graph capture owns its device buffers; the one-shot path
+// (capture false) places descriptors, tile map and counter in the calling
+// context's workspace, so no allocation happens per call once it has grown.
 int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **out, int *info) {
   Ctx *cx = ctx();
   if (!cx) return B2_ERR_NO_DEVICE;
   std::vector<GroupDesc> descs;
+  std::vector<int> map;
   long long total = 0;
-  int rc = build_descs(count, problems, descs, &total, info);
+  int rc = build_descs(count, problems, descs, map, &total, info);
   if (rc != B2_OK) return rc;
   Plan *p = new Plan();
   p->device = cx->device;
@@ -343,15 +359,31 @@ int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **o
   if (per_sm < 1) per_sm = 1;
   const long long want = (long long)cx->sm_count * per_sm;
   p->grid = (int)(total < want ? (total > 0 ? total : 1) : want);
-  if (cudaMalloc(&p->d_desc, sizeof(GroupDesc) * (descs.empty() ? 1 : descs.size())) != cudaSuccess ||
-      cudaMalloc(&p->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
-    (void)cudaGetLastError();
-    free_plan(p);
-    return B2_ERR_NOMEM;
+  const size_t bd = sizeof(GroupDesc) * (descs.empty() ? 1 : descs.size());
+  const size_t bm = sizeof(int) * (map.empty() ? 1 : map.size());
+  const size_t od = 0, om = (bd + 255) / 256 * 256, oc = om + (bm + 255) / 256 * 256;
+  if (capture) {
+    if (cudaMalloc(&p->d_desc, bd) != cudaSuccess || cudaMalloc(&p->d_map, bm) != cudaSuccess ||
+        cudaMalloc(&p->d_counter, sizeof(unsigned long long)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      free_plan(p);
+      return B2_ERR_NOMEM;
+    }
+  } else {
+    char *w = (char *)workspace(cx, WS_GROUP, oc + 256);
+    if (!w) {
+      free_plan(p);
+      return B2_ERR_NOMEM;
+    }
+    p->owns = false;
+    p->d_desc = (GroupDesc *)(w + od);
+    p->d_map = (int *)(w + om);
+    p->d_counter = (unsigned long long *)(w + oc);
   }
-  if (!descs.empty() &&
-      cudaMemcpy(p->d_desc, descs.data(), sizeof(GroupDesc) * descs.size(),
-                 cudaMemcpyHostToDevice) != cudaSuccess) {
+  if ((!descs.empty() && cudaMemcpy(p->d_desc, descs.data(), sizeof(GroupDesc) * descs.size(),
+                                    cudaMemcpyHostToDevice) != cudaSuccess) ||
+      (!map.empty() && cudaMemcpy(p->d_map, map.data(), sizeof(int) * map.size(),
+                                  cudaMemcpyHostToDevice) != cudaSuccess)) {
     free_plan(p);
     return cuda_fail(cudaGetLastError(), "grouped descriptors");
   }
@@ -384,7 +416,7 @@ int grouped_device(int count, const b2_gemm_problem *problems, cudaStream_t s, i
   int rc = make_plan(count, problems, false, &p, info);
   if (rc != B2_OK) return rc;
   rc = enqueue(*p, s);
-  // the descriptor buffer must outlive the launch
+  // the workspace holding the descriptors is reused by the next call
   cudaStreamSynchronize(s);
   free_plan(p);
   return rc;
