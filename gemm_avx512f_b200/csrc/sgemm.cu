@@ -25,7 +25,9 @@ namespace {
 // matches the 128 FMAs per clock) and forms the broadcast pairs (a, a) in
 // registers.  Storing A duplicated in shared memory instead (one 16-byte load
 // giving two pairs) cost 96 bytes per 64 FMAs and made the kernel
-// shared-memory bound (ncu at 4096^3: L1 84 % busy, FMA pipe 55 %).
+// shared-memory bound (ncu at 4096^3: L1 84 % busy, FMA pipe 55 %).  Two CTAs
+// per SM (128 registers, a few bytes spilled) beat one CTA with 150 registers:
+// 54.4 against 51.3 TFLOPS at 8192^3, 52.6 against 49.0 at 4096^3.
 constexpr int S2_M = 128, S2_N = 128, S2_K = 16, S2_APAD = 4, S2_BPAD = 4;
 constexpr int S2_ALD = S2_M + S2_APAD;  // floats per k row of the A panel
 constexpr int S2_BLD = S2_N + S2_BPAD;
@@ -56,7 +58,7 @@ __device__ __forceinline__ float4 load4(const float *p, int lim) {
 }
 
 template <bool TA, bool TB, bool VEC>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, 2)
     sgemm_ffma2_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, int lda,
                        const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
                        int ldc) {
