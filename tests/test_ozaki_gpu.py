@@ -183,3 +183,44 @@ def test_explicit_modulus_count_is_kept_for_heavy_tails(cuda):
                           slices=s)
         _lib.lib().b2_ozaki_last_plan(plan, 2)
         assert plan[0] == s
+
+
+@pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T")])
+def test_overlapped_row_and_column_blocks(cuda, ta, tb):
+    """Products large enough for the overlapped schedule run C in row blocks of
+    A and column blocks of B (here 2 x 2 ragged blocks: m = 8492 -> 4352 + 4140
+    rows, n = 4173 -> 2304 + 1869 columns) on two streams.  Against the plain
+    FP64 path on the same device inputs, with alpha/beta and a NaN planted in
+    one row of A and one column of B (recomputed by the direct dot product in
+    their own blocks)."""
+    import torch
+
+    m, n, k = 8492, 4173, 2000
+    g = torch.Generator(device=cuda).manual_seed(5)
+    ar, br = (m, k) if ta == "N" else (k, m), (k, n) if tb == "N" else (n, k)
+    A = (torch.rand(ar[1], ar[0], device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
+    B = (torch.rand(br[1], br[0], device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
+    C0 = torch.rand(n, m, device=cuda, dtype=torch.float64, generator=g)
+    # element (row 6000 of op(A), k = 7) and (k = 11, column 3000 of op(B))
+    if ta == "N":
+        A[7, 6000] = float("nan")
+    else:
+        A[6000, 7] = float("nan")
+    if tb == "N":
+        B[3000, 11] = float("nan")
+    else:
+        B[11, 3000] = float("nan")
+    out = {}
+    for method in ("ozaki", "fp64"):
+        C = C0.clone()
+        blas.dgemm_device(ta, tb, m, n, k, 1.25, A, ar[0], B, br[0], -0.5, C, m, method=method)
+        torch.cuda.synchronize()
+        out[method] = C.t()  # m x n
+    oz, fp = out["ozaki"], out["fp64"]
+    nan_oz, nan_fp = torch.isnan(oz), torch.isnan(fp)
+    assert torch.equal(nan_oz, nan_fp)
+    assert bool(nan_fp[6000].all()) and bool(nan_fp[:, 3000].all())
+    fin = ~nan_fp
+    den = k * U * float(torch.linalg.norm(torch.nan_to_num(A))) * float(torch.linalg.norm(torch.nan_to_num(B)))
+    err = float(torch.linalg.norm(torch.where(fin, oz - fp, torch.zeros_like(oz)))) / den
+    assert err <= 8, (ta, tb, err)
