@@ -68,9 +68,7 @@ struct Ctx {
   static constexpr size_t BOUNCE_BYTES = 64ull << 20;
   void *bounce[2] = {nullptr, nullptr};
   cudaEvent_t bounce_ev[2] = {nullptr, nullptr};
-  // Ozaki overlap: 4 A row blocks + 8 B column blocks sliced, 4 x 8 blocks
-  // multiplied, fork, 2 joins
-  static constexpr int OZ_EVENTS = 4 + 8 + 32 + 3;
+  static constexpr int OZ_EVENTS = 2 * 16 + 3;  // per block: sliced, multiplied; fork, 2 joins
   cudaStream_t oz_gemm = nullptr, oz_aux = nullptr;
   cudaEvent_t oz_ev[OZ_EVENTS] = {};
 };

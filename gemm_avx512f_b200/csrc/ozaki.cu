@@ -1093,46 +1093,29 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
     B2_CUDA_TRY(cudaGetLastError());
   }
 
-  // Overlapped schedule for large single-pass products: C in I x J blocks of
-  // about 4096 rows and columns (I = 2, J = 2 at 8192^3).  The INT8 GEMM of
-  // block (i, j) runs on a high-priority stream while the slicing of later row
-  // blocks of A and column blocks of B and the reconstruction of finished
-  // blocks run beside it on an auxiliary stream; only the norms, the first
-  // row block of A, the first column block of B and the last block's
-  // reconstruction are left exposed.  Measured at 8192^3 x 15 moduli on B200
-  // with column blocks only: 6.62 ms with 2 blocks, 6.71 with 4, 6.98 with 8
-  // (the auxiliary passes gain little beside the persistent GEMM, which leaves
-  // them few registers and little shared memory, while each block boundary
-  // adds a GEMM tail).  B2_OZAKI_BLOCKS = J (1 = no overlap, up to 8) fixes
-  // the column block count.
+  // Overlapped schedule for large single-pass products: B and C in J column
+  // blocks; the INT8 GEMM of block j (tensor-bound, little HBM traffic) runs
+  // on a high-priority stream while the slicing of later blocks and the
+  // reconstruction of earlier ones (HBM- and FP64-bound) run beside it on an
+  // auxiliary stream, so most of the auxiliary passes hide under the GEMMs.
+  // B2_OZAKI_BLOCKS = J (1 = no overlap, up to 16) fixes the block count.
   const char *jenv = getenv("B2_OZAKI_BLOCKS");
   const int jfix = jenv ? atoi(jenv) : 0;
+  // Blocks of about 4096 columns: measured at 8192^3 x 15 moduli on B200,
+  // 6.62 ms with 2 blocks, 6.71 with 4, 6.98 with 8 (the auxiliary passes
+  // gain little beside the persistent GEMM, which leaves them few registers
+  // and little shared memory, while each block boundary adds a GEMM tail).
   int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
            (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
               ? (n / 4096 < 2 ? 2 : (n / 4096 > 8 ? 8 : n / 4096))
               : 1;
-  if (J > 1 && jfix >= 1) J = jfix > 8 ? 8 : jfix;
+  if (J > 1 && jfix >= 1) J = jfix > 16 ? 16 : jfix;
   if (J > 1) {
-    const int I = m / 4096 < 1 ? 1 : (m / 4096 > 4 ? 4 : m / 4096);
     const int nb = (int)round_up((n + J - 1) / J, 256);
     const int nblk = (n + nb - 1) / nb;
-    const int mb = (int)round_up((m + I - 1) / I, 256);
-    const int mblk = (m + mb - 1) / mb;
     cudaStream_t gs = cx->oz_gemm, as = cx->oz_aux;
-    // events: [0, 4) A row block sliced, [4, 12) B column block sliced,
-    // [12, 44) block (i, j) multiplied (12 + j * 4 + i), 44 fork, 45/46 joins
+    // events: [0, 16) block sliced, [16, 32) block multiplied, 32 fork, 33/34 joins
     cudaEvent_t *ev = cx->oz_ev;
-    auto slice_a = [&](int i, cudaStream_t s2) {
-      const int i0 = i * mb, mi = m - i0 < mb ? m - i0 : mb;
-      dim3 grid((k + 63) / 64, (mi + 31) / 32);
-      B2_PROF(asr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", s2);
-      if (asr == 1)
-        slice_kernel<true><<<grid, 256, 0, s2>>>(A + i0 * asr, asr, ask, mi, k, sigA + i0, s_dev,
-                                                 Y + (long long)i0 * kp, kp, planeY);
-      else
-        slice_kernel<false><<<grid, 256, 0, s2>>>(A + i0 * asr, asr, ask, mi, k, sigA + i0, s_dev,
-                                                  Y + (long long)i0 * kp, kp, planeY);
-    };
     auto slice_b = [&](int j, cudaStream_t s2) {
       const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
       dim3 grid((k + 63) / 64, (nj + 31) / 32);
@@ -1144,57 +1127,48 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
         slice_kernel<false><<<grid, 256, 0, s2>>>(B + j0 * bsr, bsr, bsk, nj, k, tauB + j0, s_dev,
                                                   X + (long long)j0 * kp, kp, planeX);
     };
-    slice_a(0, st);
-    B2_CUDA_TRY(cudaGetLastError());
+    {
+      dim3 grid((k + 63) / 64, (m + 31) / 32);
+      B2_PROF(asr == 1 ? "ozaki_slice_rowcont" : "ozaki_slice_kcont", st);
+      if (asr == 1)
+        slice_kernel<true><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s_dev, Y, kp, planeY);
+      else
+        slice_kernel<false><<<grid, 256, 0, st>>>(A, asr, ask, m, k, sigA, s_dev, Y, kp, planeY);
+      B2_CUDA_TRY(cudaGetLastError());
+    }
     slice_b(0, st);
     B2_CUDA_TRY(cudaGetLastError());
-    B2_CUDA_TRY(cudaEventRecord(ev[44], st));  // exponents, count, first blocks sliced
-    B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[44], 0));
-    B2_CUDA_TRY(cudaStreamWaitEvent(as, ev[44], 0));
-    for (int i = 1; i < mblk; ++i) {
-      slice_a(i, as);
-      B2_CUDA_TRY(cudaGetLastError());
-      B2_CUDA_TRY(cudaEventRecord(ev[i], as));
-    }
+    B2_CUDA_TRY(cudaEventRecord(ev[32], st));  // exponents, count, A and block 0 sliced
+    B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[32], 0));
+    B2_CUDA_TRY(cudaStreamWaitEvent(as, ev[32], 0));
     for (int j = 1; j < nblk; ++j) {
       slice_b(j, as);
       B2_CUDA_TRY(cudaGetLastError());
-      B2_CUDA_TRY(cudaEventRecord(ev[4 + j], as));
-    }
-    // GEMMs column block by column block (the B block stays in L2 across the
-    // row blocks)
-    for (int j = 0; j < nblk && rc == B2_OK; ++j) {
-      const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
-      if (j > 0) B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[4 + j], 0));
-      for (int i = 0; i < mblk && rc == B2_OK; ++i) {
-        const int i0 = i * mb, mi = m - i0 < mb ? m - i0 : mb;
-        if (j == 0 && i > 0) B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[i], 0));
-        ResidueEpi epi{Rb + (long long)j0 * mp + i0, planeR, (int)mp, nj, mi, 0};
-        rc = run_i8_gemm(g_oz_variant, X + (long long)j0 * kp, Y + (long long)i0 * kp, k, nj, mi,
-                         s_max, kp, planeX, planeY, epi, cx->device, cx->sm_count, cx->derr, gs,
-                         s_dev);
-        if (rc == B2_OK)
-          rc = cudaEventRecord(ev[12 + j * 4 + i], gs) == cudaSuccess ? B2_OK : B2_ERR_CUDA;
-      }
+      B2_CUDA_TRY(cudaEventRecord(ev[j], as));
     }
     for (int j = 0; j < nblk && rc == B2_OK; ++j) {
       const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
-      for (int i = 0; i < mblk && rc == B2_OK; ++i) {
-        const int i0 = i * mb, mi = m - i0 < mb ? m - i0 : mb;
-        B2_CUDA_TRY(cudaStreamWaitEvent(as, ev[12 + j * 4 + i], 0));
-        B2_PROF("ozaki_reconstruct", as);
-        launch_reconstruct(Rb + (long long)j0 * mp + i0, planeR, (int)mp, s_dev, s_base, s_max,
-                           mi, nj, sigA + i0, tauB + j0, alpha, beta, C + (long long)j0 * ldc + i0,
-                           ldc, A + i0 * asr, asr, ask, B + j0 * bsr, bsk, bsr, k, as);
-        B2_CUDA_TRY(cudaGetLastError());
-      }
+      if (j > 0) B2_CUDA_TRY(cudaStreamWaitEvent(gs, ev[j], 0));
+      ResidueEpi epi{Rb + (long long)j0 * mp, planeR, (int)mp, nj, m, 0};
+      rc = run_i8_gemm(g_oz_variant, X + (long long)j0 * kp, Y, k, nj, m, s_max, kp, planeX,
+                       planeY, epi, cx->device, cx->sm_count, cx->derr, gs, s_dev);
+      if (rc == B2_OK) rc = cudaEventRecord(ev[16 + j], gs) == cudaSuccess ? B2_OK : B2_ERR_CUDA;
+    }
+    for (int j = 0; j < nblk && rc == B2_OK; ++j) {
+      const int j0 = j * nb, nj = n - j0 < nb ? n - j0 : nb;
+      B2_CUDA_TRY(cudaStreamWaitEvent(as, ev[16 + j], 0));
+      B2_PROF("ozaki_reconstruct", as);
+      launch_reconstruct(Rb + (long long)j0 * mp, planeR, (int)mp, s_dev, s_base, s_max, m, nj,
+                         sigA, tauB + j0, alpha, beta, C + (long long)j0 * ldc, ldc, A, asr, ask,
+                         B + j0 * bsr, bsk, bsr, k, as);
+      B2_CUDA_TRY(cudaGetLastError());
     }
     // join: the caller's stream waits for both streams (also on an error, so
     // nothing of this call is left running unordered)
-    cudaError_t e1 = cudaEventRecord(ev[45], as);
-    if (e1 == cudaSuccess) e1 = cudaStreamWaitEvent(st, ev[45], 0);
-    cudaError_t e2 = cudaEventRecord(ev[46], gs);
-    if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(st, ev[46], 0);
+    cudaError_t e1 = cudaEventRecord(ev[33], as);
+    if (e1 == cudaSuccess) e1 = cudaStreamWaitEvent(st, ev[33], 0);
+    cudaError_t e2 = cudaEventRecord(ev[34], gs);
+    if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(st, ev[34], 0);
     if (rc != B2_OK) return rc;
     if (e1 != cudaSuccess) return cuda_fail(e1, "ozaki overlap join");
     if (e2 != cudaSuccess) return cuda_fail(e2, "ozaki overlap join");

@@ -186,13 +186,12 @@ def test_explicit_modulus_count_is_kept_for_heavy_tails(cuda):
 
 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("T", "T")])
-def test_overlapped_row_and_column_blocks(cuda, ta, tb):
-    """Products large enough for the overlapped schedule run C in row blocks of
-    A and column blocks of B (here 2 x 2 ragged blocks: m = 8492 -> 4352 + 4140
-    rows, n = 4173 -> 2304 + 1869 columns) on two streams.  Against the plain
-    FP64 path on the same device inputs, with alpha/beta and a NaN planted in
-    one row of A and one column of B (recomputed by the direct dot product in
-    their own blocks)."""
+def test_overlapped_column_blocks_ragged(cuda, ta, tb):
+    """Products large enough for the overlapped schedule run C in column
+    blocks of B on two streams (here 2 ragged blocks: n = 4173 -> 2304 + 1869
+    columns, m = 8492 rows).  Against the plain FP64 path on the same device
+    inputs, with alpha/beta and a NaN planted in one row of A and one column of
+    B (recomputed by the direct dot product inside their blocks)."""
     import torch
 
     m, n, k = 8492, 4173, 2000
