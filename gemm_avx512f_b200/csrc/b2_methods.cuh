@@ -73,6 +73,11 @@ int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const f
                      const SgCfg &cfg, cudaStream_t s);
 int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *A, int lda,
                const float *B, int ldb, float beta, float *C, int ldc, cudaStream_t s);
+// 3xTF32 operand split (sgemm_tc.cu): the R x K view X (element (r, k) at
+// X[r*sr + k*sk]) as R rows of [big | small] TF32 segments of kp floats each
+// (row pitch 2 kp floats), the layout the tensor-core engine reads.
+int sgemm_split_tf32x3(const float *X, long long sr, long long sk, int R, int K, int kp,
+                       float *out, cudaStream_t s);
 
 // Blocked triangular solve (trsm.cu).
 int dtrsm_device(char side, char uplo, char transa, char diag, int m, int n, double alpha,

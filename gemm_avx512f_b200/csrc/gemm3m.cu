@@ -24,6 +24,7 @@
 
 #include "b2_methods.cuh"
 #include "b2_profile.cuh"
+#include "umma.cuh"
 
 namespace b2 {
 namespace {
@@ -516,6 +517,83 @@ int gemm3m_three_gemms(char ta, char tb, int m, int n, int k, T ar, T ai, T br, 
   return B2_OK;
 }
 
+// cgemm3m in ONE tensor-core GEMM launch: the three real products of the 3M
+// method run as 3xTF32 on the single-CTA tcgen05 engine in its three-
+// accumulator mode -- each work unit is a 128 x 64 tile of C that multiplies
+// batch 0 (Br, Ar), 1 (Bi, Ai) and 2 (Br + Bi, Ar + Ai) of the split operands
+// into three TMEM accumulators (two sets, 384 of 512 columns, so the epilogue
+// of a tile overlaps the next tile's MMAs), and the epilogue forms
+// Re = P1 - P2, Im = P3 - P1 - P2 and C = alpha (Re + i Im) + beta C from
+// them, so P1/P2/P3 never leave the SM.  The pre-adds (and conjugation /
+// transposition) and the TF32 big/small splits stay passes in front.
+struct C3MEpi {
+  float *C;
+  int ldc;
+  int M, N;  // C is M x N; the engine's P runs over N, Q over M
+  float ar, ai, br, bi;
+  __device__ __forceinline__ void operator()(int p, int q0, const uint32_t (&v0)[32],
+                                             const uint32_t (&v1)[32],
+                                             const uint32_t (&v2)[32]) const {
+    if (p >= N || q0 >= M) return;
+    const int nq = min(32, M - q0);
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (j < nq)
+        epilogue3m<float>(C, ldc, q0 + j, p, __uint_as_float(v0[j]), __uint_as_float(v1[j]),
+                          __uint_as_float(v2[j]), ar, ai, br, bi);
+  }
+};
+
+int cgemm3m_fused_tc(char ta, char tb, int m, int n, int k, float ar, float ai, float br,
+                     float bi, const float *A, int lda, const float *B, int ldb, float *C,
+                     int ldc, cudaStream_t s) {
+  Ctx *cx = ctx();
+  if (!cx) return B2_ERR_NO_DEVICE;
+  const bool tA = !(ta == 'N' || ta == 'n' || ta == 'R' || ta == 'r');
+  const bool tB = !(tb == 'N' || tb == 'n' || tb == 'R' || tb == 'r');
+  const float sA = (ta == 'C' || ta == 'c' || ta == 'R' || ta == 'r') ? -1.f : 1.f;
+  const float sB = (tb == 'C' || tb == 'c' || tb == 'R' || tb == 'r') ? -1.f : 1.f;
+  const long long pa = (long long)m * k, pb = (long long)k * n;
+  float *W = (float *)workspace(cx, WS_3M, (size_t)(3 * pa + 3 * pb) * sizeof(float));
+  if (!W) return B2_ERR_NOMEM;
+  float *Ar = W, *Ai = Ar + pa, *As = Ai + pa;
+  float *Br = As + pa, *Bi = Br + pb, *Bs = Bi + pb;
+  {
+    B2_PROF("gemm3m_prep", s);
+    dim3 ga((unsigned)((m + 255) / 256), (unsigned)(k < 4096 ? k : 4096));
+    prep3m_kernel<float><<<ga, 256, 0, s>>>(A, lda, tA, sA, m, k, Ar, Ai, As);
+    dim3 gb((unsigned)((k + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
+    prep3m_kernel<float><<<gb, 256, 0, s>>>(B, ldb, tB, sB, k, n, Br, Bi, Bs);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
+  // split planes: Y[t] = rows of op(A) parts (m x [big|small]), X[t] = columns
+  // of op(B) parts (n x [big|small]), t = 0, 1, 2 the three products
+  const int kp = (int)((k + 31) / 32 * 32);
+  const long long ks = 2LL * kp;
+  float *Yp = (float *)workspace(cx, WS_SPLIT_Y, (size_t)(3 * m * ks) * sizeof(float));
+  float *Xp = (float *)workspace(cx, WS_SPLIT_X, (size_t)(3 * n * ks) * sizeof(float));
+  if (!Yp || !Xp) return B2_ERR_NOMEM;
+  const float *Ya[3] = {Ar, Ai, As}, *Xb[3] = {Br, Bi, Bs};
+  for (int t = 0; t < 3; ++t) {
+    int rc = sgemm_split_tf32x3(Ya[t], 1, m, m, k, kp, Yp + t * m * ks, s);
+    if (rc == B2_OK) rc = sgemm_split_tf32x3(Xb[t], k, 1, n, k, kp, Xp + t * n * ks, s);
+    if (rc != B2_OK) return rc;
+  }
+  CUtensorMap tmX, tmY;
+  int rc = umma::make_kmajor_map(&tmX, umma::KIND_TF32, Xp, ks, n, 3, ks * 4, (long long)n * ks * 4,
+                                 umma::BM);
+  if (rc == B2_OK)
+    rc = umma::make_kmajor_map(&tmY, umma::KIND_TF32, Yp, ks, m, 3, ks * 4, (long long)m * ks * 4, 64);
+  if (rc != B2_OK) return rc;
+  // three-term interleave as in the 3xTF32 SGEMM: terms (Bb, Ab), (Bs, Ab), (Bb, As)
+  const int seg_kb = kp * 4 / umma::KBLOCK_BYTES;
+  C3MEpi epi{C, ldc, m, n, ar, ai, br, bi};
+  return umma::launch<umma::KIND_TF32, 64, 8, C3MEpi, 3>(tmX, tmY, n, m, 3LL * kp, 3, epi,
+                                                         cx->sm_count, cx->derr, s,
+                                                         "cgemm3m_umma", 0, nullptr, 1, seg_kb,
+                                                         0x2u, 0x4u);
+}
+
 template <typename T>
 int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T *A, int lda,
                   const T *B, int ldb, const T *beta, T *C, int ldc, cudaStream_t s) {
@@ -557,8 +635,21 @@ int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T
       return launch_zgemm3m_dmma<false, false>(m, n, k, A, lda, B, ldb, C, ldc, ar, ai, br, bi, sA, sB, s);
     }
   }
-  if ((double)m * n * k >= 16777216.0)
+  if ((double)m * n * k >= 16777216.0) {
+    if constexpr (sizeof(T) == 4) {
+      // one tensor-core launch once its 128 x 64 tiles fill the SMs
+      // (B2_C3M_FUSED=0 keeps the three separate GEMMs)
+      static const bool fused_on = [] {
+        const char *e = getenv("B2_C3M_FUSED");
+        return !(e && e[0] == '0');
+      }();
+      Ctx *cx = ctx();
+      const long long tiles = (long long)((n + 127) / 128) * ((m + 63) / 64);
+      if (fused_on && cx && tiles >= cx->sm_count)
+        return cgemm3m_fused_tc(ta, tb, m, n, k, ar, ai, br, bi, A, lda, B, ldb, C, ldc, s);
+    }
     return gemm3m_three_gemms<T>(ta, tb, m, n, k, ar, ai, br, bi, A, lda, B, ldb, C, ldc, s);
+  }
   dim3 grid((m + G_BM - 1) / G_BM, (n + G_BN - 1) / G_BN);
   const int smem = (int)(12 * G_BK * G_LD * sizeof(T));
   if constexpr (sizeof(T) == 8) {

@@ -247,6 +247,11 @@ int run_split(const float *Xp, long long sr, long long sk, int R, int K, int kp,
 
 }  // namespace
 
+int sgemm_split_tf32x3(const float *X, long long sr, long long sk, int R, int K, int kp,
+                       float *out, cudaStream_t s) {
+  return run_split<float>(X, sr, sk, R, K, kp, 2, 0x2u, out, s);
+}
+
 // Tensor-core engine of an SGEMM call: 0 = single CTA, 128 x 256 tile, 4
 // stages; 1 = single CTA, 128 x 128 tile, 6 stages; 2 = CTA pair, 256 x 256
 // tile, 6 stages.  split: K ranges (0 = chosen from the tile count).

@@ -280,12 +280,24 @@ __device__ __forceinline__ void tile_coords(const Problem &pr, int t, int &b, in
   tq = rr / gp;
 }
 
-template <int KIND, int BN, int STAGES, class Epi>
+// TMEM columns of an allocation: a power of two, at least 32.
+__host__ __device__ constexpr int tmem_cols(int need) {
+  return need <= 32 ? 32 : need <= 64 ? 64 : need <= 128 ? 128 : need <= 256 ? 256 : 512;
+}
+
+// NACC = 1: every (batch, tile, K range) is its own work unit.  NACC > 1: a
+// work unit is a tile, and the unit multiplies batches 0 .. NACC-1 of the
+// operands into NACC accumulators that its epilogue receives together
+// (epi(p, q0, v0, v1, v2) for NACC = 3: the three real products of the 3M
+// method); no split-K.
+template <int KIND, int BN, int STAGES, class Epi, int NACC = 1>
 __global__ void __launch_bounds__(THREADS, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap tmX,
                      const __grid_constant__ CUtensorMap tmY, const Problem pr, const Epi epi) {
   using L = SmemLayout<BN, STAGES>;
-  static_assert(2 * BN <= 512, "two accumulators must fit in TMEM");
+  static_assert(2 * NACC * BN <= 512, "two sets of accumulators must fit in TMEM");
+  static_assert(NACC == 1 || NACC == 3, "one accumulator, or three for the 3M products");
+  constexpr int TCOLS = tmem_cols(2 * NACC * BN);
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -301,7 +313,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nbatch = pr.nbatch_dev ? min(*pr.nbatch_dev, pr.nbatch) : pr.nbatch;
-  const int total_tiles = pr.tiles_p * pr.tiles_q * nbatch;
+  const int total_tiles = pr.tiles_p * pr.tiles_q * (NACC == 1 ? nbatch : 1);
   // work units: (tile, K range) pairs, the K range innermost
   const int total_units = total_tiles * pr.ksplit;
 
@@ -324,7 +336,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(2 * BN));
+                 "r"(TCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -345,7 +357,10 @@ __global__ void __launch_bounds__(THREADS, 1)
         int b, tp, tq;
         tile_coords(pr, t, b, tp, tq);
         const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
-        for (int kb = kb0; kb < kb1; ++kb) {
+        // NACC > 1: the unit's batches one after another, each over the K range
+        for (int kbb = kb0; kbb < kb0 + NACC * (kb1 - kb0) && ok; ++kbb) {
+          if (NACC > 1) b = (kbb - kb0) / (kb1 - kb0);
+          const int kb = NACC > 1 ? kb0 + (kbb - kb0) % (kb1 - kb0) : kbb;
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, pr.derr, pr.wait_ns)) {
             ok = false;
             break;
@@ -386,8 +401,10 @@ __global__ void __launch_bounds__(THREADS, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-        for (int kb = kb0; kb < kb1; ++kb) {
+        for (int kbb = kb0; kbb < kb0 + NACC * (kb1 - kb0); ++kbb) {
+          const int bi = NACC > 1 ? (kbb - kb0) / (kb1 - kb0) : 0;
+          const int kb = NACC > 1 ? kb0 + (kbb - kb0) % (kb1 - kb0) : kbb;
+          const uint32_t d_tmem = tmem_base + (uint32_t)((acc * NACC + bi) * BN);
           if (!mbar_wait(full_bar(stage), phase, abort_flag, pr.derr, pr.wait_ns)) {
             ok = false;
             break;
@@ -424,13 +441,25 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (!__all_sync(0xffffffffu, ok)) break;  // keep the warp converged for tcgen05.ld
       tc_fence_after();
       const int p = tp * BM + quarter * 32 + lane;
-      const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN);
+      const uint32_t taddr =
+          tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * NACC * BN);
 #pragma unroll 1
       for (int c = 0; c < BN / 32; ++c) {
-        uint32_t v[32];
-        tmem_ld32(taddr + (uint32_t)(c * 32), v);
-        tmem_ld_wait(v);
-        epi(b * pr.ksplit + ks, p, tq * BN + c * 32, v);  // batch x K range
+        if constexpr (NACC == 1) {
+          uint32_t v[32];
+          tmem_ld32(taddr + (uint32_t)(c * 32), v);
+          tmem_ld_wait(v);
+          epi(b * pr.ksplit + ks, p, tq * BN + c * 32, v);  // batch x K range
+        } else {
+          uint32_t v0[32], v1[32], v2[32];
+          tmem_ld32(taddr + (uint32_t)(c * 32), v0);
+          tmem_ld32(taddr + (uint32_t)(BN + c * 32), v1);
+          tmem_ld32(taddr + (uint32_t)(2 * BN + c * 32), v2);
+          tmem_ld_wait(v0);
+          tmem_ld_wait(v1);
+          tmem_ld_wait(v2);
+          epi(p, tq * BN + c * 32, v0, v1, v2);
+        }
       }
       tc_fence_before();
       __syncwarp();
@@ -456,7 +485,7 @@ __global__ void __launch_bounds__(THREADS, 1)
   if (warp == 1) {
     __syncwarp();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                 "r"(2 * BN));
+                 "r"(TCOLS));
   }
 }
 
@@ -789,11 +818,12 @@ __global__ void __launch_bounds__(THREADS, 1)
 int make_kmajor_map(CUtensorMap *map, int kind, const void *base, long long kelems, long long rows,
                     long long nbatch, long long row_bytes, long long plane_bytes, int box_rows);
 
-template <int KIND, int BN, int STAGES, class Epi>
+template <int KIND, int BN, int STAGES, class Epi, int NACC = 1>
 int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long long kelems,
            int nbatch, const Epi &epi, int sm_count, int *derr, cudaStream_t s,
            const char *prof_name, int max_ctas = 0, const int *nbatch_dev = nullptr,
            int ksplit = 1, int seg_kb = 0, unsigned seg_x = 0, unsigned seg_y = 0) {
+  if (NACC > 1 && (ksplit > 1 || nbatch != NACC || nbatch_dev)) return B2_ERR_ARG;
   using L = SmemLayout<BN, STAGES>;
   Problem pr;
   pr.P = P;
@@ -816,11 +846,12 @@ int launch(const CUtensorMap &tmX, const CUtensorMap &tmY, int P, int Q, long lo
   pr.kb_per_split = (pr.kblocks + ksplit - 1) / ksplit;
   pr.ksplit = pr.kb_per_split > 0 ? (pr.kblocks + pr.kb_per_split - 1) / pr.kb_per_split : 1;
   if (pr.ksplit < 1) pr.ksplit = 1;
-  const long long total = (long long)pr.tiles_p * pr.tiles_q * nbatch * pr.ksplit;
-  if (total <= 0) return B2_OK;
+  const long long total =
+      (long long)pr.tiles_p * pr.tiles_q * (NACC == 1 ? nbatch : 1) * pr.ksplit;
+  if (total <= 0 || (NACC > 1 && pr.kblocks <= 0)) return B2_OK;
   int grid = (int)(total < sm_count ? total : sm_count);
   if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
-  auto kern = umma_gemm_kernel<KIND, BN, STAGES, Epi>;
+  auto kern = umma_gemm_kernel<KIND, BN, STAGES, Epi, NACC>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::TOTAL);
   if (e != cudaSuccess) return cuda_fail(e, "umma smem attribute");
   B2_PROF(prof_name, s);

@@ -123,3 +123,38 @@ def test_zgemm3m_three_gemm_path_large(cuda, ta, tb):
     den = n * u * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B)) * abs(al)
     err = float(torch.linalg.norm(got - ref)) / den
     assert err <= 8, (ta, tb, err)
+
+
+@pytest.mark.parametrize("ta,tb,m,n,k", [("N", "N", 2048, 1024, 512), ("C", "T", 1100, 2100, 333),
+                                         ("R", "C", 4096, 640, 96)])
+def test_cgemm3m_one_tensor_core_launch(cuda, ta, tb, m, n, k):
+    """Once its 128 x 64 tiles fill the SMs, cgemm3m runs its three 3xTF32
+    products in one tcgen05 launch with three TMEM accumulators and combines
+    them in the epilogue (ragged tiles, conjugated and transposed operands,
+    complex alpha and beta): against the complex128 product of torch on the
+    device, FP32-class error."""
+    import torch
+
+    g = torch.Generator(device=cuda).manual_seed(m + n + k)
+    ar_, ac_ = (m, k) if ta in "NR" else (k, m)
+    br_, bc_ = (k, n) if tb in "NR" else (n, k)
+
+    def cplx(r, c):
+        return torch.complex(torch.rand(c, r, device=cuda, generator=g) * 2 - 1,
+                             torch.rand(c, r, device=cuda, generator=g) * 2 - 1)
+
+    A, B = cplx(ar_, ac_), cplx(br_, bc_)  # tensors hold the column-major matrices transposed
+    C0 = cplx(m, n)
+    op = {"N": lambda x: x, "T": lambda x: x.t(), "C": lambda x: x.conj().t(),
+          "R": lambda x: x.conj()}
+    al, be = 0.75 - 1.25j, 0.5 + 0.25j
+    Am, Bm = A.t().to(torch.complex128), B.t().to(torch.complex128)
+    ref = al * (op[ta](Am) @ op[tb](Bm)) + be * C0.t().to(torch.complex128)
+    C = C0.clone()
+    blas.cgemm3m_device(ta, tb, m, n, k, al, A, ar_, B, br_, be, C, m)
+    torch.cuda.synchronize()
+    got = C.t().to(torch.complex128)
+    u = 2.0 ** -24
+    den = k * u * float(torch.linalg.norm(Am)) * float(torch.linalg.norm(Bm)) * abs(al)
+    err = float(torch.linalg.norm(got - ref)) / den
+    assert err <= 8, (ta, tb, m, n, k, err)
