@@ -295,9 +295,13 @@ __global__ void __launch_bounds__(THREADS, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap tmX,
                      const __grid_constant__ CUtensorMap tmY, const Problem pr, const Epi epi) {
   using L = SmemLayout<BN, STAGES>;
-  static_assert(2 * NACC * BN <= 512, "two sets of accumulators must fit in TMEM");
+  // accumulator sets: two (the epilogue of a unit overlaps the next unit's
+  // MMAs) when they fit in TMEM's 512 columns, else one
+  constexpr int SETS = 2 * NACC * BN <= 512 ? 2 : 1;
+  static_assert(NACC * BN <= 512, "one set of accumulators must fit in TMEM");
   static_assert(NACC == 1 || NACC == 3, "one accumulator, or three for the 3M products");
-  constexpr int TCOLS = tmem_cols(2 * NACC * BN);
+  static_assert(NACC == 3 || SETS == 2, "the single-accumulator engine double-buffers");
+  constexpr int TCOLS = tmem_cols(SETS * NACC * BN);
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -394,8 +398,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       for (int u = blockIdx.x; u < total_units && ok; u += gridDim.x, ++it) {
         const int ks = u % pr.ksplit;
         const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
-        const int acc = it & 1;
-        const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+        const int acc = it % SETS;
+        const uint32_t acc_phase = (uint32_t)((it / SETS) & 1);
         if (!mbar_wait(tempty_bar(acc), acc_phase ^ 1u, abort_flag, pr.derr, pr.wait_ns)) {
           ok = false;
           break;
@@ -435,9 +439,9 @@ __global__ void __launch_bounds__(THREADS, 1)
       const int t = u / pr.ksplit, ks = u - t * pr.ksplit;
       int b, tp, tq;
       tile_coords(pr, t, b, tp, tq);
-      const int acc = it & 1;
+      const int acc = it % SETS;
       const bool ok =
-          mbar_wait(tfull_bar(acc), (uint32_t)((it >> 1) & 1), abort_flag, pr.derr, pr.wait_ns);
+          mbar_wait(tfull_bar(acc), (uint32_t)((it / SETS) & 1), abort_flag, pr.derr, pr.wait_ns);
       if (!__all_sync(0xffffffffu, ok)) break;  // keep the warp converged for tcgen05.ld
       tc_fence_after();
       const int p = tp * BM + quarter * 32 + lane;

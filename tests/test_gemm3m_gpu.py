@@ -125,28 +125,23 @@ def test_zgemm3m_three_gemm_path_large(cuda, ta, tb):
     assert err <= 8, (ta, tb, err)
 
 
-@pytest.mark.parametrize("ta,tb,m,n,k", [("N", "N", 2048, 1024, 512), ("C", "T", 1100, 2100, 333),
-                                         ("R", "C", 4096, 640, 96)])
-def test_cgemm3m_one_tensor_core_launch(cuda, ta, tb, m, n, k):
-    """Once its 128 x 64 tiles fill the SMs, cgemm3m runs its three 3xTF32
-    products in one tcgen05 launch with three TMEM accumulators and combines
-    them in the epilogue (ragged tiles, conjugated and transposed operands,
-    complex alpha and beta): against the complex128 product of torch on the
-    device, FP32-class error."""
-    import torch
-
+_FUSED_SCRIPT = """
+import os, sys
+sys.path.insert(0, ROOT)
+import torch
+from gemm_avx512f_b200 import _lib, blas
+cuda = torch.device("cuda:0")
+_lib.profile_enable(True)
+op = {"N": lambda x: x, "T": lambda x: x.t(), "C": lambda x: x.conj().t(), "R": lambda x: x.conj()}
+for ta, tb, m, n, k in [("N", "N", 2048, 2048, 256), ("C", "T", 1100, 2100, 333),
+                        ("R", "C", 4096, 640, 96)]:
     g = torch.Generator(device=cuda).manual_seed(m + n + k)
     ar_, ac_ = (m, k) if ta in "NR" else (k, m)
     br_, bc_ = (k, n) if tb in "NR" else (n, k)
-
     def cplx(r, c):
         return torch.complex(torch.rand(c, r, device=cuda, generator=g) * 2 - 1,
                              torch.rand(c, r, device=cuda, generator=g) * 2 - 1)
-
-    A, B = cplx(ar_, ac_), cplx(br_, bc_)  # tensors hold the column-major matrices transposed
-    C0 = cplx(m, n)
-    op = {"N": lambda x: x, "T": lambda x: x.t(), "C": lambda x: x.conj().t(),
-          "R": lambda x: x.conj()}
+    A, B, C0 = cplx(ar_, ac_), cplx(br_, bc_), cplx(m, n)
     al, be = 0.75 - 1.25j, 0.5 + 0.25j
     Am, Bm = A.t().to(torch.complex128), B.t().to(torch.complex128)
     ref = al * (op[ta](Am) @ op[tb](Bm)) + be * C0.t().to(torch.complex128)
@@ -154,7 +149,33 @@ def test_cgemm3m_one_tensor_core_launch(cuda, ta, tb, m, n, k):
     blas.cgemm3m_device(ta, tb, m, n, k, al, A, ar_, B, br_, be, C, m)
     torch.cuda.synchronize()
     got = C.t().to(torch.complex128)
-    u = 2.0 ** -24
-    den = k * u * float(torch.linalg.norm(Am)) * float(torch.linalg.norm(Bm)) * abs(al)
-    err = float(torch.linalg.norm(got - ref)) / den
-    assert err <= 8, (ta, tb, m, n, k, err)
+    den = k * 2.0 ** -24 * float(torch.linalg.norm(Am)) * float(torch.linalg.norm(Bm)) * abs(al)
+    print("ERR", ta, tb, m, n, k, float(torch.linalg.norm(got - ref)) / den, flush=True)
+print("KERNELS", " ".join(sorted(_lib.profile_report())), flush=True)
+"""
+
+
+def test_cgemm3m_one_tensor_core_launch(cuda, tmp_path):
+    """With B2_C3M_FUSED=1 (read once per process, so in a child process) and
+    128 x 128 tiles that fill the SMs, cgemm3m runs its three 3xTF32 products
+    in one tcgen05 launch with three TMEM accumulators and combines them in
+    the epilogue: ragged tiles, conjugated and transposed operands, complex
+    alpha and beta, against the complex128 product of torch on the device,
+    FP32-class error."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    script = tmp_path / "c3m_fused.py"
+    script.write_text(f"ROOT = {root!r}\n" + _FUSED_SCRIPT)
+    env = dict(os.environ, B2_C3M_FUSED="1")
+    r = subprocess.run([sys.executable, str(script)], capture_output=True, text=True,
+                       timeout=300, cwd=root, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    errs = [line.split() for line in r.stdout.splitlines() if line.startswith("ERR")]
+    assert len(errs) == 3, r.stdout
+    for e in errs:
+        assert float(e[-1]) <= 8, e
+    kernels = [line for line in r.stdout.splitlines() if line.startswith("KERNELS")][0].split()
+    assert "cgemm3m_umma" in kernels and "sgemm_umma_tf32" not in kernels, kernels
