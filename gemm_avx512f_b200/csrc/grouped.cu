@@ -26,6 +26,8 @@ namespace b2 {
 namespace {
 
 constexpr int GT_M = 64, GT_N = 64, GT_K = 16;
+constexpr int GT_NE = GT_M * GT_K / 256;  // elements of each operand panel per thread
+constexpr int GT_MINB = 3;                 // resident CTAs per SM
 constexpr int GT_LD = GT_M + 4;  // [k][m] stride (68 = 4 mod 16 doubles)
 
 struct GroupDesc {
@@ -71,7 +73,7 @@ __device__ __forceinline__ void panel_slot(int idx, bool kcont, int &mn, int &kk
 
 template <typename T>
 struct PanelRegs {
-  T a[4], b[4];
+  T a[GT_NE], b[GT_NE];
 };
 
 template <typename T>
@@ -80,7 +82,7 @@ __device__ __forceinline__ void load_panel(const GroupDesc &g, int m0, int n0, i
   const T *A = (const T *)g.A;
   const T *B = (const T *)g.B;
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
+  for (int e = 0; e < GT_NE; ++e) {
     const int idx = threadIdx.x + 256 * e;
     int mm, kk;
     panel_slot<T>(idx, g.ta != 0, mm, kk);
@@ -101,7 +103,7 @@ template <typename T>
 __device__ __forceinline__ void store_panel(const GroupDesc &g, const PanelRegs<T> &r, T *As,
                                             T *Bs) {
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
+  for (int e = 0; e < GT_NE; ++e) {
     const int idx = threadIdx.x + 256 * e;
     int mm, kk;
     panel_slot<T>(idx, g.ta != 0, mm, kk);
@@ -114,6 +116,7 @@ __device__ __forceinline__ void store_panel(const GroupDesc &g, const PanelRegs<
 
 constexpr int GT_PANEL = GT_K * GT_LD;  // elements of one operand panel
 constexpr int GT_STAGE = 2 * GT_PANEL;  // A and B panels of one stage
+constexpr int GT_SMEM = 2 * GT_STAGE * (int)sizeof(double);
 
 // Runs the K loop of one tile over two shared-memory stages; `mac(As, Bs)`
 // multiplies one resident panel pair.
@@ -233,10 +236,10 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
 // a binary search of dependent descriptor loads).  Thread 0 fetches the next
 // tile index while the current tile runs, so the counter's round trip is
 // hidden too.
-__global__ void __launch_bounds__(256, 3)
+__global__ void __launch_bounds__(256, GT_MINB)
     grouped_kernel(const GroupDesc *__restrict__ d, const int *__restrict__ tile_prob,
                    long long total_tiles, unsigned long long *counter) {
-  __shared__ __align__(16) double sm[2 * GT_STAGE];  // two stages of A and B panels
+  extern __shared__ __align__(16) double sm[];  // two stages of A and B panels (GT_SMEM)
   __shared__ long long next_s;
   if (threadIdx.x == 0) next_s = (long long)atomicAdd(counter, 1ull);
   __syncthreads();
@@ -322,7 +325,7 @@ int enqueue(const Plan &p, cudaStream_t s) {
   B2_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned long long), s));
   if (p.total_tiles == 0) return B2_OK;
   B2_PROF("grouped_gemm", s);
-  grouped_kernel<<<p.grid, 256, 0, s>>>(p.d_desc, p.d_map, p.total_tiles, p.d_counter);
+  grouped_kernel<<<p.grid, 256, GT_SMEM, s>>>(p.d_desc, p.d_map, p.total_tiles, p.d_counter);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -355,7 +358,13 @@ int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **o
   p->count = (int)descs.size();
   p->total_tiles = total;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, 256, 0);
+  if (cudaFuncSetAttribute(grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           GT_SMEM) != cudaSuccess) {
+    (void)cudaGetLastError();
+    free_plan(p);
+    return B2_ERR_CUDA;
+  }
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, 256, GT_SMEM);
   if (per_sm < 1) per_sm = 1;
   const long long want = (long long)cx->sm_count * per_sm;
   p->grid = (int)(total < want ? (total > 0 ? total : 1) : want);
