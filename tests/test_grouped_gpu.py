@@ -92,3 +92,58 @@ def test_grouped_rejects_bad_problem(cuda):
     L = _lib.lib()
     assert L.b2_gemm_grouped(len(arr), arr, None) == _lib.B2_ERR_ARG
     assert L.b2_last_info() == 4
+
+
+def test_grouped_edge_problems(cuda):
+    """Empty problems (M or N = 0) are skipped, K = 0 and alpha = 0 only
+    scale C by beta (beta = 0 keeps a NaN already in C, as dgemm_ does), and
+    the tile map and next-tile prefetch still hand every remaining tile out
+    once: a batch where most problems are degenerate, around ragged real ones."""
+    import torch
+
+    rng = np.random.default_rng(9)
+    shapes = [(0, 5, 7), (37, 0, 9), (65, 70, 0), (64, 64, 64), (1, 1, 1), (130, 3, 257),
+              (129, 65, 33), (50, 40, 0), (3, 200, 129)]
+    probs, keep = [], []
+    for i, (m, n, k) in enumerate(shapes * 3):
+        dtype = i % 2
+        npdt = np.float64 if dtype == 0 else np.float32
+        ta, tb = ("N", "T")[i % 2], ("N", "T")[(i // 2) % 2]
+        ar, ac = (m, k) if ta == "N" else (k, m)
+        br, bc = (k, n) if tb == "N" else (n, k)
+        a = np.asfortranarray(rng.uniform(-1, 1, (max(ar, 1), max(ac, 1))).astype(npdt))
+        b = np.asfortranarray(rng.uniform(-1, 1, (max(br, 1), max(bc, 1))).astype(npdt))
+        c = np.asfortranarray(rng.uniform(-1, 1, (max(m, 1), max(n, 1))).astype(npdt))
+        al = 0.0 if i == 13 else 1.25
+        be = 0.0 if i % 3 == 0 else -0.5
+        if m > 0 and n > 0 and be == 0.0:
+            c[0, 0] = np.nan  # beta == 0 still multiplies C: the NaN stays
+        da, db, dc = (torch.from_numpy(x.T.copy()).to(cuda) for x in (a, b, c))
+        probs.append(_lib.GemmProblem(dtype, ta.encode(), tb.encode(), m, n, k, al, be,
+                                      da.data_ptr(), max(ar, 1), db.data_ptr(), max(br, 1),
+                                      dc.data_ptr(), max(m, 1)))
+        keep.append((a, b, c, dc, ta, tb, m, n, k, al, be))
+    arr = (_lib.GemmProblem * len(probs))(*probs)
+    L = _lib.lib()
+    assert L.b2_gemm_grouped(len(probs), arr, None) == 0
+    torch.cuda.synchronize()
+    for (a, b, c, dc, ta, tb, m, n, k, al, be) in keep:
+        got = np.asfortranarray(dc.cpu().numpy().T)
+        if m == 0 or n == 0:
+            assert np.array_equal(got, c, equal_nan=True)
+            continue
+        ar = m if ta == "N" else k
+        br = k if tb == "N" else n
+        if k == 0 or al == 0.0:
+            ref = a.dtype.type(be) * c  # only beta C (0 * NaN stays NaN)
+        else:
+            ref = c.copy(order="F")
+            O.gemm(ta, tb, m, n, k, a.dtype.type(al), a[:ar], b[:br], a.dtype.type(be), ref)
+        assert np.array_equal(np.isnan(got), np.isnan(ref)), (m, n, k, be)
+        fin = ~np.isnan(ref)
+        u = np.finfo(a.dtype).eps / 2
+        if k == 0 or al == 0.0:
+            assert np.allclose(got[fin], ref[fin], rtol=0, atol=4 * u), (m, n, k)
+        else:
+            g, r = np.where(fin, got, 0), np.where(fin, ref, 0)
+            assert normalized(g, r, k, a[:ar], b[:br], u) <= 8, (a.dtype, m, n, k, ta, tb)
