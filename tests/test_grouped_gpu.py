@@ -122,12 +122,12 @@ def test_grouped_edge_problems(cuda):
         probs.append(_lib.GemmProblem(dtype, ta.encode(), tb.encode(), m, n, k, al, be,
                                       da.data_ptr(), max(ar, 1), db.data_ptr(), max(br, 1),
                                       dc.data_ptr(), max(m, 1)))
-        keep.append((a, b, c, dc, ta, tb, m, n, k, al, be))
+        keep.append((a, b, c, dc, ta, tb, m, n, k, al, be, da, db))  # device buffers stay alive
     arr = (_lib.GemmProblem * len(probs))(*probs)
     L = _lib.lib()
     assert L.b2_gemm_grouped(len(probs), arr, None) == 0
     torch.cuda.synchronize()
-    for (a, b, c, dc, ta, tb, m, n, k, al, be) in keep:
+    for (a, b, c, dc, ta, tb, m, n, k, al, be, _, _) in keep:
         got = np.asfortranarray(dc.cpu().numpy().T)
         if m == 0 or n == 0:
             assert np.array_equal(got, c, equal_nan=True)
