@@ -361,10 +361,12 @@ __global__ void __launch_bounds__(THREADS, 1)
         int b, tp, tq;
         tile_coords(pr, t, b, tp, tq);
         const int kb0 = ks * pr.kb_per_split, kb1 = min(pr.kblocks, kb0 + pr.kb_per_split);
-        // NACC > 1: the unit's batches one after another, each over the K range
+        // NACC > 1: the unit's batches interleaved per K block (the three
+        // products of a K block back to back, so the operand panels of all
+        // batches stay in L2 together)
         for (int kbb = kb0; kbb < kb0 + NACC * (kb1 - kb0) && ok; ++kbb) {
-          if (NACC > 1) b = (kbb - kb0) / (kb1 - kb0);
-          const int kb = NACC > 1 ? kb0 + (kbb - kb0) % (kb1 - kb0) : kbb;
+          if (NACC > 1) b = (kbb - kb0) % NACC;
+          const int kb = NACC > 1 ? kb0 + (kbb - kb0) / NACC : kbb;
           if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, pr.derr, pr.wait_ns)) {
             ok = false;
             break;
@@ -406,8 +408,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         tc_fence_after();
         for (int kbb = kb0; kbb < kb0 + NACC * (kb1 - kb0); ++kbb) {
-          const int bi = NACC > 1 ? (kbb - kb0) / (kb1 - kb0) : 0;
-          const int kb = NACC > 1 ? kb0 + (kbb - kb0) % (kb1 - kb0) : kbb;
+          const int bi = NACC > 1 ? (kbb - kb0) % NACC : 0;
+          const int kb = NACC > 1 ? kb0 + (kbb - kb0) / NACC : kbb;
           const uint32_t d_tmem = tmem_base + (uint32_t)((acc * NACC + bi) * BN);
           if (!mbar_wait(full_bar(stage), phase, abort_flag, pr.derr, pr.wait_ns)) {
             ok = false;
