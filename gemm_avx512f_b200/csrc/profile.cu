@@ -103,10 +103,14 @@ int b2_profile_timeline(char *buf, int len) {
         cudaEventElapsedTime(&b, t0, r.b) == cudaSuccess) {
       if (buf && len > 0 && off < len) {
         int w = snprintf(buf + off, (size_t)(len - off), "%s %.6f %.6f\n", r.name, a, b);
-        if (w > 0 && off + w < len) off += w;
-        else off = len;
+        if (w > 0 && off + w < len) {
+          off += w;
+          ++n;
+        } else {
+          buf[off] = 0;  // the line did not fit: drop it and stop listing
+          off = len;
+        }
       }
-      ++n;
     } else {
       (void)cudaGetLastError();
     }

@@ -408,8 +408,8 @@ B2_API int b2_profile_enable(int on);
 B2_API int b2_profile_report(char *buf, int len);
 /* The same records as a timeline: one line "name start_ms end_ms" per launch
  * in issue order, times relative to the first record's start (launches on
- * different streams may overlap); clears the records and returns how many
- * launches were listed. */
+ * different streams may overlap); lines that do not fit in buf are dropped
+ * whole.  Clears the records and returns how many launches were listed. */
 B2_API int b2_profile_timeline(char *buf, int len);
 
 #ifdef __cplusplus
