@@ -68,7 +68,7 @@ struct Ctx {
   static constexpr size_t BOUNCE_BYTES = 64ull << 20;
   void *bounce[2] = {nullptr, nullptr};
   cudaEvent_t bounce_ev[2] = {nullptr, nullptr};
-  static constexpr int OZ_EVENTS = 2 * 16 + 3;  // per block: sliced, multiplied; fork, 2 joins
+  static constexpr int OZ_EVENTS = 2 * 16 + 3;  // per block: sliced, multiplied; fork, 2 joins (the last two also join the norm passes)
   cudaStream_t oz_gemm = nullptr, oz_aux = nullptr;
   cudaEvent_t oz_ev[OZ_EVENTS] = {};
 };

@@ -1080,10 +1080,28 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   int *plan_word = (int *)((uint8_t *)cx->pinned + 64);
   int *plan_dev = cx->pinned_dev ? (int *)((uint8_t *)cx->pinned_dev + 64) : nullptr;
   if (adaptive) B2_CUDA_TRY(cudaMemsetAsync(stat, 0, 4 * sizeof(double), st));
-  if (!reuse_a)
-    rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
-  if (rc == B2_OK)
-    rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, scrB, adaptive ? stat + 2 : nullptr, st);
+  // Large single-pass products overlap the GEMMs with the auxiliary passes on
+  // a second stream (below); their two norm passes, both HBM-bound, also run
+  // side by side there (separate scratch and statistics).
+  const bool overlap = !piped && !rows_view && kchunks == 1 && n >= 4096 &&
+                       (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx);
+  if (overlap && !reuse_a) {
+    cudaStream_t as = cx->oz_aux;
+    B2_CUDA_TRY(cudaEventRecord(cx->oz_ev[33], st));
+    B2_CUDA_TRY(cudaStreamWaitEvent(as, cx->oz_ev[33], 0));
+    rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, scrB, adaptive ? stat + 2 : nullptr, as);
+    const int ra = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
+    // join before anything can return, so no work of this call stays unordered
+    cudaError_t e = cudaEventRecord(cx->oz_ev[34], as);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, cx->oz_ev[34], 0);
+    if (rc == B2_OK) rc = ra;
+    if (rc == B2_OK && e != cudaSuccess) rc = cuda_fail(e, "ozaki norm join");
+  } else {
+    if (!reuse_a)
+      rc = norm_exponents(A, asr, ask, m, k, t.H, sigA, scrA, adaptive ? stat : nullptr, st);
+    if (rc == B2_OK)
+      rc = norm_exponents(B, bsr, bsk, n, k, t.H, tauB, scrB, adaptive ? stat + 2 : nullptr, st);
+  }
   if (rc != B2_OK) return rc;
   {
     B2_PROF("ozaki_decide", st);
@@ -1105,10 +1123,7 @@ int dgemm_ozaki(char ta, char tb, int m, int n, int k, double alpha, const doubl
   // 6.62 ms with 2 blocks, 6.71 with 4, 6.98 with 8 (the auxiliary passes
   // gain little beside the persistent GEMM, which leaves them few registers
   // and little shared memory, while each block boundary adds a GEMM tail).
-  int J = (!piped && !rows_view && kchunks == 1 && n >= 4096 &&
-           (double)m * n * k >= 8589934592.0 && ozaki_overlap_streams(cx))
-              ? (n / 4096 < 2 ? 2 : (n / 4096 > 8 ? 8 : n / 4096))
-              : 1;
+  int J = overlap ? (n / 4096 < 2 ? 2 : (n / 4096 > 8 ? 8 : n / 4096)) : 1;
   if (J > 1 && jfix >= 1) J = jfix > 16 ? 16 : jfix;
   if (J > 1) {
     const int nb = (int)round_up((n + J - 1) / J, 256);

@@ -96,11 +96,26 @@ int b2_profile_report(char *buf, int len) {
 int b2_profile_timeline(char *buf, int len) {
   int n = 0, off = 0;
   if (buf && len > 0) buf[0] = 0;
+  // Launches on two streams can start in another order than they were
+  // recorded: times count from the earliest start of all.
   cudaEvent_t t0 = g_prof.recs.empty() ? nullptr : g_prof.recs.front().a;
-  for (auto &r : g_prof.recs) {
-    float a = 0.f, b = 0.f;
-    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&a, t0, r.a) == cudaSuccess &&
-        cudaEventElapsedTime(&b, t0, r.b) == cudaSuccess) {
+  std::vector<float> at(g_prof.recs.size(), 0.f), bt(g_prof.recs.size(), 0.f);
+  std::vector<char> ok(g_prof.recs.size(), 0);
+  float first = 0.f;
+  for (size_t i = 0; i < g_prof.recs.size(); ++i) {
+    const Rec &r = g_prof.recs[i];
+    if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&at[i], t0, r.a) == cudaSuccess &&
+        cudaEventElapsedTime(&bt[i], t0, r.b) == cudaSuccess) {
+      ok[i] = 1;
+      if (at[i] < first) first = at[i];
+    } else {
+      (void)cudaGetLastError();
+    }
+  }
+  for (size_t i = 0; i < g_prof.recs.size(); ++i) {
+    const Rec &r = g_prof.recs[i];
+    if (ok[i]) {
+      const float a = at[i] - first, b = bt[i] - first;
       if (buf && len > 0 && off < len) {
         int w = snprintf(buf + off, (size_t)(len - off), "%s %.6f %.6f\n", r.name, a, b);
         if (w > 0 && off + w < len) {
@@ -111,8 +126,6 @@ int b2_profile_timeline(char *buf, int len) {
           off = len;
         }
       }
-    } else {
-      (void)cudaGetLastError();
     }
   }
   for (auto &r : g_prof.recs) {

@@ -407,8 +407,9 @@ B2_API long long b2_launch_count(void);
 B2_API int b2_profile_enable(int on);
 B2_API int b2_profile_report(char *buf, int len);
 /* The same records as a timeline: one line "name start_ms end_ms" per launch
- * in issue order, times relative to the first record's start (launches on
- * different streams may overlap); lines that do not fit in buf are dropped
+ * in issue order, times relative to the earliest start among the records
+ * (launches on different streams may overlap, and a later-issued launch may
+ * start first); lines that do not fit in buf are dropped
  * whole.  Clears the records and returns how many launches were listed. */
 B2_API int b2_profile_timeline(char *buf, int len);
 

@@ -34,6 +34,7 @@ def test_report_and_timeline_of_an_overlapped_ozaki_call(cuda):
     assert names.count("ozaki_i8_gemm") == 2  # one INT8 GEMM per column block
     assert names.count("ozaki_reconstruct") == 2
     assert names[0].startswith("ozaki_norm")
+    assert min(a for _, a, _ in tl) == 0.0  # times count from the earliest start
     assert all(0.0 <= a <= b for _, a, b in tl)
     gemms = [(a, b) for nm, a, b in tl if nm == "ozaki_i8_gemm"]
     assert gemms[0][1] <= gemms[1][0] + 1e-3  # the GEMMs run one after another
