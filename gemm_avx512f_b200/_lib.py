@@ -36,7 +36,8 @@ class GemmProblem(C.Structure):
                 ("m", C.c_int), ("n", C.c_int), ("k", C.c_int),
                 ("alpha", C.c_double), ("beta", C.c_double),
                 ("A", C.c_void_p), ("lda", C.c_int), ("B", C.c_void_p), ("ldb", C.c_int),
-                ("C", C.c_void_p), ("ldc", C.c_int)]
+                ("C", C.c_void_p), ("ldc", C.c_int),
+                ("alpha_i", C.c_double), ("beta_i", C.c_double)]
 
 
 class B2Error(RuntimeError):

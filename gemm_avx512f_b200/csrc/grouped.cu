@@ -7,10 +7,13 @@
 // the host flattens every problem into 64 x 64 output tiles (problems sorted
 // by K, largest first, so the longest tiles are handed out first), a
 // persistent grid pulls tile indices from a device-side atomic counter, finds
-// the owning problem by binary search over the tile prefix sums and runs the
-// tile with the problem's own dtype, transposes, strides and alpha/beta:
+// the owning problem through a tile -> problem map and runs the tile with the
+// problem's own dtype, transposes, strides and alpha/beta:
 //   FP64 tiles: DMMA mma.sync.m16n8k8.f64, 8 warps of 32 x 16;
-//   FP32 tiles: FFMA, 256 threads of 4 x 4.
+//   FP32 tiles: FFMA, 8 warps of 32 x 16, each lane 4 x 4;
+//   complex tiles (zgemm3m_ / cgemm3m_ problems): 32 x 32, the three real
+//   products of the 3M method on DMMA (complex128) or FFMA (complex64);
+// warps whose block of a tile lies outside the problem skip their multiplies.
 // A plan uploads the descriptors once and captures "reset counter + launch" in
 // a CUDA graph, so replaying a batch is a single graph launch.
 #include <stdlib.h>
@@ -36,10 +39,12 @@ struct GroupDesc {
   void *C;
   double alpha, beta;
   int m, n, k, lda, ldb, ldc;
-  int dtype;  // 0 = f64, 1 = f32
+  int dtype;  // 0 = f64, 1 = f32, 2 = complex128 3M, 3 = complex64 3M
   int ta, tb;
   int tiles_m, tiles_n;
   long long tile_offset;
+  double alpha_i, beta_i;  // complex dtypes
+  int ca, cb;              // complex dtypes: operand conjugated ('C', 'R')
 };
 
 // A GT_K-deep panel: op(A) tile (64 x 16) and op(B) tile (16 x 64), 4
@@ -58,11 +63,11 @@ struct GroupDesc {
 // Its shared-memory stores then hit every bank pair at most twice per warp
 // (stride 68: bank pair (8k + 2m) mod 32 for doubles, bank (4k + m) mod 32
 // for floats), where one k column of 16 k by 2 rows had hit each four times.
-template <typename T>
+template <typename T, int W = GT_M>
 __device__ __forceinline__ void panel_slot(int idx, bool kcont, int &mn, int &kk) {
   if (!kcont) {
-    mn = idx % GT_M;
-    kk = idx / GT_M;
+    mn = idx % W;
+    kk = idx / W;
     return;
   }
   constexpr int KL = 32 / (int)sizeof(T);  // 4 doubles or 8 floats: one 32-byte sector
@@ -153,8 +158,14 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
     for (int j = 0; j < 2; ++j)
 #pragma unroll
       for (int v = 0; v < 4; ++v) acc[i][j][v] = 0.0;
+  // A warp whose 32 x 16 block lies wholly outside the problem (edge tiles of
+  // small M or N) skips its multiplies: the test depends on the warp and the
+  // tile only, so every lane of the warp takes the same branch.  (Skipping
+  // single 16 x 8 blocks as well spills registers and was slower.)
+  const bool live = m0 + wm0 < g.m && n0 + wn0 < g.n;
   // DMMA m16n8k8: A fragment rows g, g+8 x k t, t+4; B fragment k t, t+4 x column g
   tile_k_loop<double>(g, m0, n0, sm, [&](const double *As, const double *Bs) {
+    if (!live) return;
 #pragma unroll
     for (int kk = 0; kk < GT_K; kk += 8) {
       double af[2][4], bf[2][2];
@@ -198,18 +209,25 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
       }
 }
 
+// FP32 tile: 8 warps of 32 x 16 outputs (the FP64 warp grid), each lane 4 x 4
+// of them: rows 32 (warp / 4) + 4 (lane % 8) + i, columns 16 (warp % 4) +
+// 4 (lane / 8) + j.  A warp whose block lies wholly outside the problem skips
+// its multiplies.
 __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rm = (warp >> 2) * 32 + (lane & 7) * 4, cn = (warp & 3) * 16 + (lane >> 3) * 4;
+  const bool live = m0 + (warp >> 2) * 32 < g.m && n0 + (warp & 3) * 16 < g.n;
   float acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
   tile_k_loop<float>(g, m0, n0, sm, [&](const float *As, const float *Bs) {
+    if (!live) return;
 #pragma unroll
     for (int kk = 0; kk < GT_K; ++kk) {
-      const float4 a = *reinterpret_cast<const float4 *>(&As[kk * GT_LD + tx * 4]);
-      const float4 b = *reinterpret_cast<const float4 *>(&Bs[kk * GT_LD + ty * 4]);
+      const float4 a = *reinterpret_cast<const float4 *>(&As[kk * GT_LD + rm]);
+      const float4 b = *reinterpret_cast<const float4 *>(&Bs[kk * GT_LD + cn]);
       const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -224,7 +242,7 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int m = m0 + tx * 4 + i, n = n0 + ty * 4 + j;
+      const int m = m0 + rm + i, n = n0 + cn + j;
       if (m < g.m && n < g.n) {
         float *p = C + (long long)n * g.ldc + m;
         *p = one ? fmaf(al, acc[i][j], *p) : fmaf(al, acc[i][j], be * *p);
@@ -232,14 +250,246 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
     }
 }
 
+// ------------------------------------------------------------ 3M tiles --
+// A complex problem's tile is 32 x 32 outputs of C.  Each K panel holds op(A)
+// (32 x 16) and op(B) (16 x 32) complex elements, two of each per thread,
+// de-interleaved on the way to shared memory into two real panels per
+// operand: real part and imaginary part (negated for a conjugated operand).
+// Every warp forms the three real products of the 3M method on one 16 x 8
+// block, the pre-added operands of the third from the first two's fragments
+// in registers (two shared loads fewer per product than a third panel),
+//     P1 = Ar Br,  P2 = Ai Bi,  P3 = (Ar + Ai)(Br + Bi),
+// and the epilogue combines Re = P1 - P2, Im = P3 - P1 - P2 with the complex
+// alpha and beta.  The reference kernels (zgemm3m_kernel_2x8_skylakex.c:
+// 336-351, cgemm3m_kernel_16x4_skylakex.c:415-440) take one pre-added real
+// product per call; here the three share the staged panels and one queue
+// entry.
+constexpr int Z_T = 32;                  // tile edge
+constexpr int Z_LD = Z_T + 4;            // panel row stride (36 = 4 mod 16)
+constexpr int Z_PANEL = GT_K * Z_LD;     // one real panel
+constexpr int Z_STAGE = 4 * Z_PANEL;     // A: re, im; B: re, im
+constexpr int Z_PER = Z_T * GT_K / 256;  // complex elements per thread per operand
+constexpr int GT_SMEM_3M = 2 * Z_STAGE * (int)sizeof(double);
+
+// The slot map takes the complex element as its unit (16 or 8 bytes), so a
+// K-contiguous operand is still read one whole 32-byte sector per row.
+template <typename R>
+struct Cplx;
+template <>
+struct Cplx<double> {
+  using type = double2;
+};
+template <>
+struct Cplx<float> {
+  using type = float2;
+};
+
+template <typename R>
+struct Panel3M {
+  R ar[Z_PER], ai[Z_PER], br[Z_PER], bi[Z_PER];
+};
+
+template <typename R>
+__device__ __forceinline__ void load_panel3m(const GroupDesc &g, int m0, int n0, int k0,
+                                             Panel3M<R> &r) {
+  using CT = typename Cplx<R>::type;
+  const R *A = (const R *)g.A;
+  const R *B = (const R *)g.B;
+  const R sa = g.ca ? (R)-1 : (R)1, sb = g.cb ? (R)-1 : (R)1;
+#pragma unroll
+  for (int e = 0; e < Z_PER; ++e) {
+    const int idx = threadIdx.x + 256 * e;
+    int mm, kk;
+    panel_slot<CT, Z_T>(idx, g.ta != 0, mm, kk);
+    const int gm = m0 + mm, gk = k0 + kk;
+    R re = 0, im = 0;
+    if (gm < g.m && gk < g.k) {
+      const R *q = A + 2 * (g.ta ? (long long)gm * g.lda + gk : (long long)gk * g.lda + gm);
+      re = q[0];
+      im = sa * q[1];
+    }
+    r.ar[e] = re;
+    r.ai[e] = im;
+    int nn, kb;
+    panel_slot<CT, Z_T>(idx, g.tb == 0, nn, kb);
+    const int gn = n0 + nn, gk2 = k0 + kb;
+    re = 0;
+    im = 0;
+    if (gn < g.n && gk2 < g.k) {
+      const R *q = B + 2 * (g.tb ? (long long)gk2 * g.ldb + gn : (long long)gn * g.ldb + gk2);
+      re = q[0];
+      im = sb * q[1];
+    }
+    r.br[e] = re;
+    r.bi[e] = im;
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ void store_panel3m(const GroupDesc &g, const Panel3M<R> &r, R *S) {
+  using CT = typename Cplx<R>::type;
+#pragma unroll
+  for (int e = 0; e < Z_PER; ++e) {
+    const int idx = threadIdx.x + 256 * e;
+    int mm, kk;
+    panel_slot<CT, Z_T>(idx, g.ta != 0, mm, kk);
+    R *a = S + kk * Z_LD + mm;
+    a[0] = r.ar[e];
+    a[Z_PANEL] = r.ai[e];
+    int nn, kb;
+    panel_slot<CT, Z_T>(idx, g.tb == 0, nn, kb);
+    R *b = S + 2 * Z_PANEL + kb * Z_LD + nn;
+    b[0] = r.br[e];
+    b[Z_PANEL] = r.bi[e];
+  }
+}
+
+// K loop of a 3M tile over two stages; `mac(S)` multiplies one resident stage.
+template <typename R, class Mac>
+__device__ __forceinline__ void tile3m_k_loop(const GroupDesc &g, int m0, int n0, R *buf,
+                                              Mac mac) {
+  const int nk = (g.k + GT_K - 1) / GT_K;
+  Panel3M<R> r;
+  if (nk > 0) {
+    load_panel3m<R>(g, m0, n0, 0, r);
+    store_panel3m<R>(g, r, buf);
+  }
+  __syncthreads();
+  for (int it = 0; it < nk; ++it) {
+    const bool more = it + 1 < nk;
+    if (more) load_panel3m<R>(g, m0, n0, (it + 1) * GT_K, r);
+    mac(buf + (it & 1) * Z_STAGE);
+    if (more) store_panel3m<R>(g, r, buf + ((it + 1) & 1) * Z_STAGE);
+    __syncthreads();  // the stage just read is refilled two iterations later
+  }
+}
+
+// C(m, n) = alpha (Re + i Im) + beta C(m, n) with Re = P1 - P2 and
+// Im = P3 - P1 - P2; C is scaled whenever beta != 1 (the reference drivers'
+// rule), so a NaN in C stays even for beta = 0.
+template <typename R>
+__device__ __forceinline__ void store3m(const GroupDesc &g, int m, int n, R p1, R p2, R p3) {
+  if (m >= g.m || n >= g.n) return;
+  const R re = p1 - p2, im = p3 - p1 - p2;
+  const R ar = (R)g.alpha, ai = (R)g.alpha_i, br = (R)g.beta, bi = (R)g.beta_i;
+  R *c = (R *)g.C + 2 * ((long long)n * g.ldc + m);
+  R cr = c[0], ci = c[1];
+  if (!(br == (R)1 && bi == (R)0)) {
+    const R tr = br * cr - bi * ci, ti = br * ci + bi * cr;
+    cr = tr;
+    ci = ti;
+  }
+  c[0] = cr + (ar * re - ai * im);
+  c[1] = ci + (ar * im + ai * re);
+}
+
+// complex128 3M tile: 8 warps of 16 x 8 outputs (2 x 4 of them), one DMMA
+// m16n8k8 block per product per K step of 8.
+__device__ void tile_z3m(const GroupDesc &g, int m0, int n0, double *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gq = lane >> 2, t = lane & 3;
+  const int wm0 = (warp >> 2) * 16, wn0 = (warp & 3) * 8;
+  const bool live = m0 + wm0 < g.m && n0 + wn0 < g.n;
+  double acc[3][4];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[p][v] = 0.0;
+  tile3m_k_loop<double>(g, m0, n0, sm, [&](const double *S) {
+    if (!live) return;
+#pragma unroll
+    for (int kk = 0; kk < GT_K; kk += 8) {
+      double af[2][4], bf[2][2];  // [re, im] fragments
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+#pragma unroll
+        for (int v1 = 0; v1 < 2; ++v1)
+#pragma unroll
+          for (int v0 = 0; v0 < 2; ++v0)
+            af[p][v0 + 2 * v1] = S[p * Z_PANEL + (kk + t + 4 * v1) * Z_LD + wm0 + gq + 8 * v0];
+#pragma unroll
+        for (int v = 0; v < 2; ++v)
+          bf[p][v] = S[(2 + p) * Z_PANEL + (kk + t + 4 * v) * Z_LD + wn0 + gq];
+      }
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        if (p == 2) {  // (Ar + Ai), (Br + Bi)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) af[0][v] += af[1][v];
+#pragma unroll
+          for (int v = 0; v < 2; ++v) bf[0][v] += bf[1][v];
+        }
+        const int q = p == 1 ? 1 : 0;
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+            "{%8,%9}, {%0,%1,%2,%3};\n"
+            : "+d"(acc[p][0]), "+d"(acc[p][1]), "+d"(acc[p][2]), "+d"(acc[p][3])
+            : "d"(af[q][0]), "d"(af[q][1]), "d"(af[q][2]), "d"(af[q][3]), "d"(bf[q][0]),
+              "d"(bf[q][1]));
+      }
+    }
+  });
+
+#pragma unroll
+  for (int v = 0; v < 4; ++v)
+    store3m<double>(g, m0 + wm0 + gq + 8 * (v >> 1), n0 + wn0 + 2 * t + (v & 1), acc[0][v],
+                    acc[1][v], acc[2][v]);
+}
+
+// complex64 3M tile: the same warp grid, each lane 2 x 2 outputs of its
+// warp's 16 x 8 block (rows 2 (lane % 8) + i, columns 2 (lane / 8) + j), FFMA.
+__device__ void tile_c3m(const GroupDesc &g, int m0, int n0, float *sm) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int rm = (warp >> 2) * 16 + (lane & 7) * 2, cn = (warp & 3) * 8 + (lane >> 3) * 2;
+  const bool live = m0 + (warp >> 2) * 16 < g.m && n0 + (warp & 3) * 8 < g.n;
+  float acc[3][2][2];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) acc[p][i][j] = 0.f;
+  tile3m_k_loop<float>(g, m0, n0, sm, [&](const float *S) {
+    if (!live) return;
+#pragma unroll
+    for (int kk = 0; kk < GT_K; ++kk) {
+      const float2 a1 = *reinterpret_cast<const float2 *>(&S[kk * Z_LD + rm]);
+      const float2 a2 = *reinterpret_cast<const float2 *>(&S[Z_PANEL + kk * Z_LD + rm]);
+      const float2 b1 = *reinterpret_cast<const float2 *>(&S[2 * Z_PANEL + kk * Z_LD + cn]);
+      const float2 b2 = *reinterpret_cast<const float2 *>(&S[3 * Z_PANEL + kk * Z_LD + cn]);
+      const float2 a3 = make_float2(a1.x + a2.x, a1.y + a2.y);
+      const float2 b3 = make_float2(b1.x + b2.x, b1.y + b2.y);
+      const float2 av[3] = {a1, a2, a3}, bv[3] = {b1, b2, b3};
+#pragma unroll
+      for (int p = 0; p < 3; ++p) {
+        acc[p][0][0] = fmaf(av[p].x, bv[p].x, acc[p][0][0]);
+        acc[p][0][1] = fmaf(av[p].x, bv[p].y, acc[p][0][1]);
+        acc[p][1][0] = fmaf(av[p].y, bv[p].x, acc[p][1][0]);
+        acc[p][1][1] = fmaf(av[p].y, bv[p].y, acc[p][1][1]);
+      }
+    }
+  });
+
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      store3m<float>(g, m0 + rm + i, n0 + cn + j, acc[0][i][j], acc[1][i][j], acc[2][i][j]);
+}
+
 // tile_prob[t] is the problem that owns flattened tile t (one load instead of
 // a binary search of dependent descriptor loads).  Thread 0 fetches the next
 // tile index while the current tile runs, so the counter's round trip is
 // hidden too.
+// CPLX: the batch holds complex (3M) problems.  Real-only batches run the
+// instantiation without the complex tiles, which keeps its registers free of
+// their code (compiled together the four tile kinds spill).
+template <bool CPLX>
 __global__ void __launch_bounds__(256, GT_MINB)
     grouped_kernel(const GroupDesc *__restrict__ d, const int *__restrict__ tile_prob,
                    long long total_tiles, unsigned long long *counter) {
-  extern __shared__ __align__(16) double sm[];  // two stages of A and B panels (GT_SMEM)
+  // two stages of A and B panels (GT_SMEM; GT_SMEM_3M when the batch has complex problems)
+  extern __shared__ __align__(16) double sm[];
   __shared__ long long next_s;
   if (threadIdx.x == 0) next_s = (long long)atomicAdd(counter, 1ull);
   __syncthreads();
@@ -249,9 +499,15 @@ __global__ void __launch_bounds__(256, GT_MINB)
     if (threadIdx.x == 0) next_s = (long long)atomicAdd(counter, 1ull);
     const GroupDesc g = d[tile_prob[t]];
     const int local = (int)(t - g.tile_offset);
-    const int m0 = (local % g.tiles_m) * GT_M, n0 = (local / g.tiles_m) * GT_N;
-    if (g.dtype == 0) tile_f64(g, m0, n0, sm);
-    else tile_f32(g, m0, n0, reinterpret_cast<float *>(sm));
+    const int tm = local % g.tiles_m, tn = local / g.tiles_m;
+    float *smf = reinterpret_cast<float *>(sm);
+    if (!CPLX || g.dtype < 2) {
+      if (g.dtype == 0) tile_f64(g, tm * GT_M, tn * GT_N, sm);
+      else tile_f32(g, tm * GT_M, tn * GT_N, smf);
+    } else {
+      if (g.dtype == 2) tile_z3m(g, tm * Z_T, tn * Z_T, sm);
+      else tile_c3m(g, tm * Z_T, tn * Z_T, smf);
+    }
     __syncthreads();  // thread 0's store of next_s is visible
     t = next_s;
   }
@@ -268,12 +524,18 @@ struct Plan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int grid = 0;
+  bool cplx = false;   // the batch holds complex problems
+  int smem = GT_SMEM;  // GT_SMEM_3M when it does
 };
 
 bool is_nt(char c) { return c == 'N' || c == 'n'; }
+// complex operands: 'N'/'R' keep the layout, 'C'/'R' conjugate
+bool is_cnt(char c) { return c == 'N' || c == 'n' || c == 'R' || c == 'r'; }
+bool is_conj(char c) { return c == 'C' || c == 'c' || c == 'R' || c == 'r'; }
 
 int build_descs(int count, const b2_gemm_problem *pr, std::vector<GroupDesc> &out,
-                std::vector<int> &map, long long *total, int *info) {
+                std::vector<int> &map, long long *total, bool *has3m, int *info) {
+  *has3m = false;
   std::vector<int> order(count);
   std::iota(order.begin(), order.end(), 0);
   // largest K first: each tile costs ~K, so the long tiles are dequeued first
@@ -283,9 +545,12 @@ int build_descs(int count, const b2_gemm_problem *pr, std::vector<GroupDesc> &ou
   for (int idx : order) {
     const b2_gemm_problem &p = pr[idx];
     int inf = 0;
-    if (p.dtype != 0 && p.dtype != 1) { *info = idx + 1; return B2_ERR_ARG; }
-    if (check_gemm(p.transa, p.transb, p.m, p.n, p.k, p.lda, p.ldb, p.ldc, p.A, p.B, p.C, &inf) !=
-        B2_OK) {
+    if (p.dtype < 0 || p.dtype > 3) { *info = idx + 1; return B2_ERR_ARG; }
+    const bool cplx = p.dtype >= 2;
+    const bool tA = cplx ? !is_cnt(p.transa) : !is_nt(p.transa);
+    const bool tB = cplx ? !is_cnt(p.transb) : !is_nt(p.transb);
+    if (check_gemm(tA ? 'T' : 'N', tB ? 'T' : 'N', p.m, p.n, p.k, p.lda, p.ldb, p.ldc, p.A, p.B,
+                   p.C, &inf) != B2_OK) {
       *info = idx + 1;
       return B2_ERR_ARG;
     }
@@ -303,10 +568,16 @@ int build_descs(int count, const b2_gemm_problem *pr, std::vector<GroupDesc> &ou
     g.ldb = p.ldb;
     g.ldc = p.ldc;
     g.dtype = p.dtype;
-    g.ta = is_nt(p.transa) ? 0 : 1;
-    g.tb = is_nt(p.transb) ? 0 : 1;
-    g.tiles_m = (p.m + GT_M - 1) / GT_M;
-    g.tiles_n = (p.n + GT_N - 1) / GT_N;
+    g.ta = tA ? 1 : 0;
+    g.tb = tB ? 1 : 0;
+    g.alpha_i = cplx ? p.alpha_i : 0.0;
+    g.beta_i = cplx ? p.beta_i : 0.0;
+    g.ca = cplx && is_conj(p.transa) ? 1 : 0;
+    g.cb = cplx && is_conj(p.transb) ? 1 : 0;
+    const int tm = cplx ? Z_T : GT_M, tn = cplx ? Z_T : GT_N;
+    g.tiles_m = (p.m + tm - 1) / tm;
+    g.tiles_n = (p.n + tn - 1) / tn;
+    if (cplx) *has3m = true;
     g.tile_offset = off;
     off += (long long)g.tiles_m * g.tiles_n;
     if (off > (1ll << 31)) { *info = idx + 1; return B2_ERR_ARG; }
@@ -325,7 +596,12 @@ int enqueue(const Plan &p, cudaStream_t s) {
   B2_CUDA_TRY(cudaMemsetAsync(p.d_counter, 0, sizeof(unsigned long long), s));
   if (p.total_tiles == 0) return B2_OK;
   B2_PROF("grouped_gemm", s);
-  grouped_kernel<<<p.grid, 256, GT_SMEM, s>>>(p.d_desc, p.d_map, p.total_tiles, p.d_counter);
+  if (p.cplx)
+    grouped_kernel<true><<<p.grid, 256, p.smem, s>>>(p.d_desc, p.d_map, p.total_tiles,
+                                                     p.d_counter);
+  else
+    grouped_kernel<false><<<p.grid, 256, p.smem, s>>>(p.d_desc, p.d_map, p.total_tiles,
+                                                      p.d_counter);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -351,20 +627,24 @@ int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **o
   std::vector<GroupDesc> descs;
   std::vector<int> map;
   long long total = 0;
-  int rc = build_descs(count, problems, descs, map, &total, info);
+  bool has3m = false;
+  int rc = build_descs(count, problems, descs, map, &total, &has3m, info);
   if (rc != B2_OK) return rc;
   Plan *p = new Plan();
   p->device = cx->device;
   p->count = (int)descs.size();
   p->total_tiles = total;
+  p->cplx = has3m;
+  p->smem = has3m ? GT_SMEM_3M : GT_SMEM;
   int per_sm = 0;
-  if (cudaFuncSetAttribute(grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           GT_SMEM) != cudaSuccess) {
+  const void *fn = has3m ? (const void *)grouped_kernel<true> : (const void *)grouped_kernel<false>;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem) !=
+      cudaSuccess) {
     (void)cudaGetLastError();
     free_plan(p);
     return B2_ERR_CUDA;
   }
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grouped_kernel, 256, GT_SMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, p->smem);
   if (per_sm < 1) per_sm = 1;
   const long long want = (long long)cx->sm_count * per_sm;
   p->grid = (int)(total < want ? (total > 0 ? total : 1) : want);

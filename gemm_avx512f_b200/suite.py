@@ -245,6 +245,31 @@ def run_grouped(ctx, out, quick):
                "graph_plan_ms": ms2, "graph_plan_tflops": flops / ms2 / 1e9,
                "per_problem_calls_ms": ms3, "speedup_vs_per_problem": ms3 / ms1})
 
+    # the same batch plus the zgemm3m 2048^3 product as 3M problem in the queue
+    n = 2048
+    ha, hb, _ = inputs.config4_complex(n)
+    Az, Bz = upload(ha, dev), upload(hb, dev)
+    del ha, hb
+    Cz = torch.zeros(n * n, dtype=torch.complex128, device=dev)
+    pz = _lib.GemmProblem(2, b"N", b"N", n, n, n, 1.0, 0.0, Az.data_ptr(), n, Bz.data_ptr(), n,
+                          Cz.data_ptr(), n)
+    arr2 = (_lib.GemmProblem * (count + 1))(pz, *probs)
+    plan = C.c_void_p()
+    assert L.b2_grouped_plan_create(count + 1, arr2, C.byref(plan)) == 0
+    ms4 = T(lambda: L.b2_grouped_plan_launch(plan, st.cuda_stream), reps=5)
+    L.b2_grouped_plan_destroy(plan)
+    ref = Az.view(n, n).t() @ Bz.view(n, n).t()
+    err = float(torch.linalg.norm(Cz.view(n, n).t() - ref) / torch.linalg.norm(ref))
+    zal = (C.c_double * 2)(1.0, 0.0)
+    zbe = (C.c_double * 2)(0.0, 0.0)
+    ms5 = T(lambda: L.b2_zgemm3m(b"N", b"N", n, n, n, C.addressof(zal), Az.data_ptr(), n,
+                                 Bz.data_ptr(), n, C.addressof(zbe), Cz.data_ptr(), n,
+                                 st.cuda_stream), reps=5)
+    emit(out, {"workload": "grouped 4096 problems + zgemm3m 2048^3 (3M problem) in one launch",
+               "graph_plan_ms": ms4, "zgemm3m_err_normwise": err,
+               "separate_ms": ms2 + ms5, "zgemm3m_alone_ms": ms5,
+               "gflop_real_issued": (flops + 6.0 * n ** 3) / 1e9})
+
 
 def run_complex(ctx, out, quick):
     torch, dev, T, P = ctx["torch"], ctx["dev"], ctx["timer"], ctx["peaks"]

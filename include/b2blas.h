@@ -273,19 +273,28 @@ B2_API int b2_dtrsm_kernel(char side, char trans, long m, long n, double *sa, do
 /* counterpart API in the reference, whose parallel drivers split one GEMM   */
 /* (src/gemm_driver.c:136-149; OpenBLAS-like_implementation/dgemm.c:449-483   */
 /* task queue); here the queue spans a whole batch.  Pointers are device     */
-/* pointers; each problem follows the dgemm_/sgemm_ contract.                */
+/* pointers; each problem follows the dgemm_/sgemm_ contract, or for the     */
+/* complex dtypes the zgemm3m_/cgemm3m_ contract: the 3M method's three real */
+/* products (zgemm3m_kernel_2x8_skylakex.c:336-351, cgemm3m_kernel_16x4_     */
+/* skylakex.c:415-440) and their pre/post additions run inside the same      */
+/* launch, one tile of C per queue entry.                                    */
 /* ------------------------------------------------------------------------ */
 typedef struct b2_gemm_problem {
-  int dtype;            /* 0 = FP64 (double), 1 = FP32 (float) */
-  char transa, transb;  /* 'N'/'n' = no transpose, anything else = transpose */
+  int dtype;            /* 0 = FP64 (double), 1 = FP32 (float), 2 = complex128
+                           (zgemm3m_), 3 = complex64 (cgemm3m_) */
+  char transa, transb;  /* real: 'N'/'n' = no transpose, anything else =
+                           transpose; complex: 'N', 'T', 'C' (conjugate
+                           transpose) or 'R' (conjugate, no transpose) */
   int m, n, k;
-  double alpha, beta;   /* rounded to float for dtype 1 */
-  const void *A;
-  int lda;
+  double alpha, beta;   /* real parts for the complex dtypes; rounded to
+                           float for dtypes 1 and 3 */
+  const void *A;        /* complex dtypes: interleaved (re, im) pairs, */
+  int lda;              /* leading dimensions in complex elements */
   const void *B;
   int ldb;
   void *C;
   int ldc;
+  double alpha_i, beta_i; /* imaginary parts of alpha and beta (dtypes 2, 3) */
 } b2_gemm_problem;
 
 /* One-shot: upload descriptors, launch, wait for the descriptors to be consumed.

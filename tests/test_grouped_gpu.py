@@ -147,3 +147,106 @@ def test_grouped_edge_problems(cuda):
         else:
             g, r = np.where(fin, got, 0), np.where(fin, ref, 0)
             assert normalized(g, r, k, a[:ar], b[:br], u) <= 8, (a.dtype, m, n, k, ta, tb)
+
+
+def test_grouped_skinny_tile_shapes(cuda):
+    """Problems with M or N far below 64 run on the 32 x 128 and 128 x 32
+    tiles, the others on 64 x 64: every shape x dtype x transpose pair, with
+    ragged edges in M, N and K, against the oracle."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    shapes = [(17, 300, 45), (300, 21, 77), (33, 129, 16), (129, 31, 130), (16, 16, 1000),
+              (64, 64, 31), (8, 1000, 9), (1000, 8, 17), (65, 33, 64)]
+    probs, keep = [], []
+    i = 0
+    for (m, n, k) in shapes:
+        for dtype in (0, 1):
+            for ta in "NT":
+                for tb in "NT":
+                    npdt = np.float64 if dtype == 0 else np.float32
+                    ar, ac = (m, k) if ta == "N" else (k, m)
+                    br, bc = (k, n) if tb == "N" else (n, k)
+                    a = np.asfortranarray(rng.uniform(-1, 1, (ar, ac)).astype(npdt))
+                    b = np.asfortranarray(rng.uniform(-1, 1, (br, bc)).astype(npdt))
+                    c = np.asfortranarray(rng.uniform(-1, 1, (m, n)).astype(npdt))
+                    al, be = (1.0, 0.0) if i % 2 else (-0.75, 1.0)
+                    da, db, dc = (torch.from_numpy(x.T.copy()).to(cuda) for x in (a, b, c))
+                    probs.append(_lib.GemmProblem(dtype, ta.encode(), tb.encode(), m, n, k, al, be,
+                                                  da.data_ptr(), ar, db.data_ptr(), br,
+                                                  dc.data_ptr(), m))
+                    keep.append((a, b, c, da, db, dc, ta, tb, al, be))
+                    i += 1
+    arr = (_lib.GemmProblem * len(probs))(*probs)
+    st = torch.cuda.Stream(cuda)
+    assert _lib.lib().b2_gemm_grouped(len(arr), arr, st.cuda_stream) == 0
+    st.synchronize()
+    check(keep)
+
+
+def test_grouped_complex_3m_problems_in_the_same_launch(cuda):
+    """zgemm3m_ / cgemm3m_ problems (dtypes 2 and 3) share the queue with real
+    ones: every op() form ('N', 'T', 'C', 'R'), complex alpha and beta,
+    ragged sizes, padded leading dimensions, K = 0, alpha = 0 and a NaN in C
+    with beta = 0, each checked against the oracle's 3M restatement (whose
+    real products are the bit-exact restatement of the reference dgemm_)."""
+    import torch
+
+    rng = np.random.default_rng(21)
+    shapes = [(13, 9, 21), (33, 65, 40), (70, 31, 129), (1, 1, 1), (64, 64, 16), (5, 40, 0),
+              (40, 5, 7), (100, 90, 70)]
+    probs, keep = [], []
+    i = 0
+    for (m, n, k) in shapes:
+        for dtype in (2, 3):
+            for ta, tb in (("N", "N"), ("T", "C"), ("C", "R"), ("R", "T")):
+                cdt = np.complex128 if dtype == 2 else np.complex64
+                ar, ac = (m, k) if ta in "NR" else (k, m)
+                br, bc = (k, n) if tb in "NR" else (n, k)
+                pa, pb, pc = 2, 1, 3  # padded leading dimensions
+
+                def cm(r, c, pad):
+                    x = rng.uniform(-1, 1, (r + pad, max(c, 1))) + 1j * rng.uniform(-1, 1, (r + pad, max(c, 1)))
+                    return np.asfortranarray(x.astype(cdt))
+
+                a, b, c = cm(ar, ac, pa), cm(br, bc, pb), cm(m, n, pc)
+                al = 0.0 if i == 5 else 0.75 - 1.25j
+                be = 0.0 if i % 4 == 1 else (1.0 if i % 4 == 2 else 0.5 + 0.25j)
+                if be == 0.0:
+                    c[0, 0] = np.nan  # beta == 0 still multiplies C: the NaN stays
+                da, db, dc = (torch.from_numpy(x.T.copy()).to(cuda) for x in (a, b, c))
+                p = _lib.GemmProblem(dtype, ta.encode(), tb.encode(), m, n, k, float(np.real(al)),
+                                     float(np.real(be)), da.data_ptr(), a.shape[0], db.data_ptr(),
+                                     b.shape[0], dc.data_ptr(), c.shape[0])
+                p.alpha_i, p.beta_i = float(np.imag(al)), float(np.imag(be))
+                probs.append(p)
+                keep.append((a, b, c, da, db, dc, ta, tb, m, n, k, al, be))
+                i += 1
+    real_arr, real_keep = make_batch(cuda, 40, 16, 150, seed=22)
+    arr = (_lib.GemmProblem * (len(probs) + len(real_arr)))(*probs, *real_arr)
+    st = torch.cuda.Stream(cuda)
+    n0 = _lib.launch_count()
+    assert _lib.lib().b2_gemm_grouped(len(arr), arr, st.cuda_stream) == 0
+    st.synchronize()
+    assert _lib.launch_count() - n0 == 1  # real and 3M problems in one launch
+    check(real_keep)
+    for (a, b, c, da, db, dc, ta, tb, m, n, k, al, be) in keep:
+        got = np.asfortranarray(dc.cpu().numpy().T)
+        ar = m if ta in "NR" else k
+        br = k if tb in "NR" else n
+        ref = c.copy(order="F")
+        if k > 0 and al != 0.0:
+            O.gemm3m(ta, tb, m, n, k, al, a[:ar], b[:br], be, ref[:m])
+        elif not (be == 1.0):
+            ref[:m, :n] = be * c[:m, :n]
+        assert np.array_equal(got[m:], c[m:], equal_nan=True), "padding rows of C were written"
+        assert np.array_equal(np.isnan(got[:m]), np.isnan(ref[:m])), (m, n, k, be)
+        fin = ~np.isnan(ref[:m])
+        u = np.finfo(a.dtype).eps / 2
+        g, r = np.where(fin, got[:m], 0), np.where(fin, ref[:m], 0)
+        den = max(k, 1) * u * np.linalg.norm(a[:ar]) * np.linalg.norm(b[:br]) + u * np.linalg.norm(r)
+        if den == 0.0:  # K = 0 and beta = 0: C is exactly zero (NaN kept above)
+            assert np.array_equal(g, r), (m, n, k, ta, tb)
+            continue
+        err = np.linalg.norm((g - r).astype(np.complex128)) / den
+        assert err <= 8, (a.dtype, m, n, k, ta, tb, err)

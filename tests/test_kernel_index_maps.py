@@ -162,9 +162,9 @@ def test_z_fragment_loads_conflict_free():
 GT_M, GT_K, GT_LD = 64, 16, 68
 
 
-def panel_slot(idx, kcont, esz):
+def panel_slot(idx, kcont, esz, W=GT_M):
     if not kcont:
-        return idx % GT_M, idx // GT_M
+        return idx % W, idx // W
     kl = 32 // esz
     lane, w = idx & 31, idx >> 5
     return lane // kl + (32 // kl) * (w // (GT_K // kl)), lane % kl + kl * (w % (GT_K // kl))
@@ -205,3 +205,70 @@ def test_grouped_kcont_loads_use_whole_sectors():
                 ks.sort()
                 assert len(ks) * esz == 32 and ks == list(range(ks[0], ks[0] + len(ks)))
                 assert (ks[0] * esz) % 32 == 0
+
+
+def test_grouped_warp_blocks_own_each_output_once_and_skip_only_outside():
+    # FP64 and FP32 tiles share the warp grid: warp w owns rows 32 (w // 4) ..
+    # + 31 and columns 16 (w % 4) .. + 15; FP32 lane l owns rows 4 (l % 8) + i,
+    # columns 4 (l // 8) + j of it.  A warp skips its multiplies when its
+    # block starts past M or N, which leaves no output of the problem behind.
+    owned = {}
+    for tid in range(256):
+        lane, warp = tid & 31, tid >> 5
+        rm, cn = (warp >> 2) * 32 + (lane & 7) * 4, (warp & 3) * 16 + (lane >> 3) * 4
+        for i in range(4):
+            for j in range(4):
+                owned[(rm + i, cn + j)] = owned.get((rm + i, cn + j), 0) + 1
+                assert (rm + i) // 32 == warp >> 2 and (cn + j) // 16 == warp & 3
+    assert len(owned) == 64 * 64 and set(owned.values()) == {1}
+    for m in (1, 16, 31, 32, 33, 63, 64):
+        for n in (1, 15, 16, 17, 48, 64):
+            for warp in range(8):
+                live = (warp >> 2) * 32 < m and (warp & 3) * 16 < n
+                inside = any(r < m and c < n for r in range((warp >> 2) * 32, (warp >> 2) * 32 + 32)
+                             for c in range((warp & 3) * 16, (warp & 3) * 16 + 16))
+                assert live == inside
+
+
+def test_grouped_3m_panels_and_warp_blocks():
+    # complex tiles: 32-wide panels of 16 k, 2 complex elements per thread per
+    # operand in slot order (element size 16 B for complex128, 8 B for
+    # complex64: K-contiguous rows read whole 32-byte sectors); warps of
+    # 16 x 8 outputs on a 2 x 4 grid; complex64 lanes own 2 x 2 of them
+    W, LD = 32, 36
+    for esz in (16, 8):
+        for kcont in (False, True):
+            seen = {panel_slot(tid + 256 * e, kcont, esz, W) for tid in range(256) for e in range(2)}
+            assert seen == {(mn, k) for mn in range(W) for k in range(GT_K)}
+            if kcont:
+                for w in range(16):
+                    rows = {}
+                    for lane in range(32):
+                        mn, k = panel_slot(32 * w + lane, True, esz, W)
+                        rows.setdefault(mn, []).append(k)
+                    for ks in rows.values():
+                        assert len(ks) * esz == 32 and sorted(ks)[0] * esz % 32 == 0
+            # real and imaginary panels are stored as 8-byte (complex128) or
+            # 4-byte (complex64) words: at most two lanes per bank (pair)
+            for w in range(16):
+                hits = {}
+                for lane in range(32):
+                    mn, k = panel_slot(32 * w + lane, kcont, esz, W)
+                    bank = ((k * LD + mn) * (esz // 8)) % 32
+                    hits[bank] = hits.get(bank, 0) + 1
+                assert max(hits.values()) <= 2, (esz, kcont, w)
+    owned = set()
+    for warp in range(8):
+        wm0, wn0 = (warp >> 2) * 16, (warp & 3) * 8
+        for lane in range(32):
+            gq, t = lane >> 2, lane & 3
+            for v in range(4):  # DMMA accumulator layout
+                owned.add((wm0 + gq + 8 * (v >> 1), wn0 + 2 * t + (v & 1)))
+    assert owned == {(m, n) for m in range(32) for n in range(32)}
+    owned = set()
+    for tid in range(256):
+        lane, warp = tid & 31, tid >> 5
+        rm, cn = (warp >> 2) * 16 + (lane & 7) * 2, (warp & 3) * 8 + (lane >> 3) * 2
+        assert rm // 16 == warp >> 2 and cn // 8 == warp & 3
+        owned |= {(rm + i, cn + j) for i in range(2) for j in range(2)}
+    assert owned == {(m, n) for m in range(32) for n in range(32)}
