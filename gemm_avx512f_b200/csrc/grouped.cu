@@ -271,8 +271,26 @@ constexpr int Z_STAGE = 4 * Z_PANEL;     // A: re, im; B: re, im
 constexpr int Z_PER = Z_T * GT_K / 256;  // complex elements per thread per operand
 constexpr int GT_SMEM_3M = 2 * Z_STAGE * (int)sizeof(double);
 
-// The slot map takes the complex element as its unit (16 or 8 bytes), so a
-// K-contiguous operand is still read one whole 32-byte sector per row.
+// Slot map of a complex panel (32 wide), in complex elements (16 or 8 bytes).
+// An operand whose m (or n) is contiguous takes m = idx % 32, k = idx / 32.  A
+// K-contiguous one takes KL = 32 B / element consecutive k per row (one whole
+// 32-byte sector) over 32 / KL rows per warp, and spreads those rows so that
+// the warp's stores into the real and imaginary panels (stride 36) find every
+// bank free: rows 0-3 and 8-11 in the first half-warp of a complex128 store
+// (one 128-byte wavefront each), rows 0-3 and 16-19 for complex64.
+template <typename CT>
+__device__ __forceinline__ void panel_slot3m(int idx, bool kcont, int &mn, int &kk) {
+  if (!kcont) {
+    mn = idx % 32;
+    kk = idx / 32;
+    return;
+  }
+  constexpr int KL = 32 / (int)sizeof(CT);  // 2 (complex128) or 4 (complex64)
+  const int lane = idx & 31, w = idx >> 5, r = lane / KL;
+  kk = lane % KL + KL * (w % (GT_K / KL));
+  const int row = KL == 2 ? ((r & 3) | ((r & 4) << 1) | ((r & 8) >> 1)) : ((r & 3) | ((r & 4) << 2));
+  mn = row + (KL == 2 ? 16 : 4) * (w / (GT_K / KL));
+}
 template <typename R>
 struct Cplx;
 template <>
@@ -300,7 +318,7 @@ __device__ __forceinline__ void load_panel3m(const GroupDesc &g, int m0, int n0,
   for (int e = 0; e < Z_PER; ++e) {
     const int idx = threadIdx.x + 256 * e;
     int mm, kk;
-    panel_slot<CT, Z_T>(idx, g.ta != 0, mm, kk);
+    panel_slot3m<CT>(idx, g.ta != 0, mm, kk);
     const int gm = m0 + mm, gk = k0 + kk;
     R re = 0, im = 0;
     if (gm < g.m && gk < g.k) {
@@ -311,7 +329,7 @@ __device__ __forceinline__ void load_panel3m(const GroupDesc &g, int m0, int n0,
     r.ar[e] = re;
     r.ai[e] = im;
     int nn, kb;
-    panel_slot<CT, Z_T>(idx, g.tb == 0, nn, kb);
+    panel_slot3m<CT>(idx, g.tb == 0, nn, kb);
     const int gn = n0 + nn, gk2 = k0 + kb;
     re = 0;
     im = 0;
@@ -332,12 +350,12 @@ __device__ __forceinline__ void store_panel3m(const GroupDesc &g, const Panel3M<
   for (int e = 0; e < Z_PER; ++e) {
     const int idx = threadIdx.x + 256 * e;
     int mm, kk;
-    panel_slot<CT, Z_T>(idx, g.ta != 0, mm, kk);
+    panel_slot3m<CT>(idx, g.ta != 0, mm, kk);
     R *a = S + kk * Z_LD + mm;
     a[0] = r.ar[e];
     a[Z_PANEL] = r.ai[e];
     int nn, kb;
-    panel_slot<CT, Z_T>(idx, g.tb == 0, nn, kb);
+    panel_slot3m<CT>(idx, g.tb == 0, nn, kb);
     R *b = S + 2 * Z_PANEL + kb * Z_LD + nn;
     b[0] = r.br[e];
     b[Z_PANEL] = r.bi[e];

@@ -230,33 +230,47 @@ def test_grouped_warp_blocks_own_each_output_once_and_skip_only_outside():
                 assert live == inside
 
 
+def panel_slot3m(idx, kcont, esz):
+    if not kcont:
+        return idx % 32, idx // 32
+    kl = 32 // esz
+    lane, w = idx & 31, idx >> 5
+    r = lane // kl
+    kk = lane % kl + kl * (w % (GT_K // kl))
+    row = ((r & 3) | ((r & 4) << 1) | ((r & 8) >> 1)) if kl == 2 else ((r & 3) | ((r & 4) << 2))
+    return row + (16 if kl == 2 else 4) * (w // (GT_K // kl)), kk
+
+
 def test_grouped_3m_panels_and_warp_blocks():
     # complex tiles: 32-wide panels of 16 k, 2 complex elements per thread per
     # operand in slot order (element size 16 B for complex128, 8 B for
-    # complex64: K-contiguous rows read whole 32-byte sectors); warps of
+    # complex64: K-contiguous rows read whole 32-byte sectors); the real and
+    # imaginary panels (stride 36) are stored as doubles (complex128: each
+    # half-warp is one 128-byte wavefront, so at most one lane per bank pair)
+    # or floats (complex64: one lane per bank in the whole warp); warps of
     # 16 x 8 outputs on a 2 x 4 grid; complex64 lanes own 2 x 2 of them
-    W, LD = 32, 36
+    LD = 36
     for esz in (16, 8):
         for kcont in (False, True):
-            seen = {panel_slot(tid + 256 * e, kcont, esz, W) for tid in range(256) for e in range(2)}
-            assert seen == {(mn, k) for mn in range(W) for k in range(GT_K)}
-            if kcont:
-                for w in range(16):
+            seen = {panel_slot3m(tid + 256 * e, kcont, esz) for tid in range(256) for e in range(2)}
+            assert seen == {(mn, k) for mn in range(32) for k in range(GT_K)}
+            for w in range(16):
+                slots = [panel_slot3m(32 * w + lane, kcont, esz) for lane in range(32)]
+                if kcont:
                     rows = {}
-                    for lane in range(32):
-                        mn, k = panel_slot(32 * w + lane, True, esz, W)
+                    for mn, k in slots:
                         rows.setdefault(mn, []).append(k)
                     for ks in rows.values():
-                        assert len(ks) * esz == 32 and sorted(ks)[0] * esz % 32 == 0
-            # real and imaginary panels are stored as 8-byte (complex128) or
-            # 4-byte (complex64) words: at most two lanes per bank (pair)
-            for w in range(16):
-                hits = {}
-                for lane in range(32):
-                    mn, k = panel_slot(32 * w + lane, kcont, esz, W)
-                    bank = ((k * LD + mn) * (esz // 8)) % 32
-                    hits[bank] = hits.get(bank, 0) + 1
-                assert max(hits.values()) <= 2, (esz, kcont, w)
+                        ks.sort()
+                        assert len(ks) * esz == 32 and ks[0] * esz % 32 == 0
+                        assert ks == list(range(ks[0], ks[0] + len(ks)))
+                if esz == 16:
+                    for half in (slots[:16], slots[16:]):
+                        pairs = [(k * LD + mn) % 16 for mn, k in half]
+                        assert len(set(pairs)) == 16, (kcont, w, pairs)
+                else:
+                    banks = [(k * LD + mn) % 32 for mn, k in slots]
+                    assert len(set(banks)) == 32, (kcont, w, banks)
     owned = set()
     for warp in range(8):
         wm0, wn0 = (warp >> 2) * 16, (warp & 3) * 8
