@@ -65,6 +65,10 @@ struct CtxOwner {
     }
     for (int i = 0; i < Ctx::OZ_EVENTS; ++i)
       if (c->oz_ev[i]) cudaEventDestroy(c->oz_ev[i]);
+    for (int i = 0; i < 2; ++i) {
+      if (c->grp_ev[i]) cudaEventSynchronize(c->grp_ev[i]), cudaEventDestroy(c->grp_ev[i]);
+      if (c->grp_host[i]) cudaFreeHost(c->grp_host[i]);
+    }
     if (c->oz_gemm) cudaStreamSynchronize(c->oz_gemm), cudaStreamDestroy(c->oz_gemm);
     if (c->oz_aux) cudaStreamSynchronize(c->oz_aux), cudaStreamDestroy(c->oz_aux);
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -33,6 +33,7 @@ enum WsSlot {
   WS_SPLIT_X, WS_SPLIT_Y,                   // SGEMM split planes
   WS_TRSM, WS_TRSM_INV, WS_TRSM_TMP, WS_3M, WS_GROUP, WS_ERR, WS_MISC,
   WS_KABI_A, WS_KABI_B, WS_KABI_D,         // kernel-ABI unpacked panels / 3M product
+  WS_GROUP2,                                // second descriptor slot of one-shot grouped calls
   WS_COUNT
 };
 
@@ -71,6 +72,14 @@ struct Ctx {
   static constexpr int OZ_EVENTS = 2 * 16 + 3;  // per block: sliced, multiplied; fork, 2 joins (the last two also join the norm passes)
   cudaStream_t oz_gemm = nullptr, oz_aux = nullptr;
   cudaEvent_t oz_ev[OZ_EVENTS] = {};
+  // One-shot grouped calls alternate two descriptor slots (device workspace
+  // WS_GROUP / WS_GROUP2, pinned host staging, and an event after the launch
+  // that last read them), so one call's descriptors are built and uploaded
+  // while the previous call's kernel runs.
+  void *grp_host[2] = {nullptr, nullptr};
+  size_t grp_host_bytes[2] = {0, 0};
+  cudaEvent_t grp_ev[2] = {nullptr, nullptr};
+  int grp_next = 0;
 };
 // The two streams and the events of the overlapped Ozaki schedule (false when
 // they cannot be created; the caller then runs the plain schedule).

@@ -17,6 +17,7 @@
 // A plan uploads the descriptors once and captures "reset counter + launch" in
 // a CUDA graph, so replaying a batch is a single graph launch.
 #include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <numeric>
@@ -637,9 +638,11 @@ void free_plan(Plan *p) {
 }
 
 // A plan for graph capture owns its device buffers; the one-shot path
-// (capture false) places descriptors, tile map and counter in the calling
-// context's workspace, so no allocation happens per call once it has grown.
-int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **out, int *info) {
+// (capture false) places descriptors, tile map and counter in one of the
+// calling context's two descriptor slots (`*slot`), uploads them on `s` from
+// pinned staging, and allocates nothing per call once the slots have grown.
+int make_plan(int count, const b2_gemm_problem *problems, bool capture, cudaStream_t s, Plan **out,
+              int *slot, int *info) {
   Ctx *cx = ctx();
   if (!cx) return B2_ERR_NO_DEVICE;
   std::vector<GroupDesc> descs;
@@ -677,20 +680,56 @@ int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **o
       return B2_ERR_NOMEM;
     }
   } else {
-    char *w = (char *)workspace(cx, WS_GROUP, oc + 256);
+    // The slot's previous launch (two calls ago) has read its descriptors.
+    const int sl = cx->grp_next;
+    cx->grp_next ^= 1;
+    *slot = sl;
+    if (cx->grp_ev[sl]) {
+      const cudaError_t e = cudaEventSynchronize(cx->grp_ev[sl]);
+      if (e != cudaSuccess) {
+        free_plan(p);
+        return cuda_fail(e, "grouped descriptor slot");
+      }
+    } else if (cudaEventCreateWithFlags(&cx->grp_ev[sl], cudaEventDisableTiming) != cudaSuccess) {
+      cx->grp_ev[sl] = nullptr;
+      free_plan(p);
+      return cuda_fail(cudaGetLastError(), "grouped descriptor event");
+    }
+    char *w = (char *)workspace(cx, sl ? WS_GROUP2 : WS_GROUP, oc + 256);
     if (!w) {
       free_plan(p);
       return B2_ERR_NOMEM;
     }
+    if (cx->grp_host_bytes[sl] < oc) {
+      if (cx->grp_host[sl]) cudaFreeHost(cx->grp_host[sl]);
+      cx->grp_host[sl] = nullptr;
+      cx->grp_host_bytes[sl] = 0;
+      if (cudaHostAlloc(&cx->grp_host[sl], oc, cudaHostAllocDefault) != cudaSuccess) {
+        (void)cudaGetLastError();
+        cx->grp_host[sl] = nullptr;
+        free_plan(p);
+        return B2_ERR_NOMEM;
+      }
+      cx->grp_host_bytes[sl] = oc;
+    }
+    char *h = (char *)cx->grp_host[sl];
+    if (!descs.empty()) memcpy(h + od, descs.data(), sizeof(GroupDesc) * descs.size());
+    if (!map.empty()) memcpy(h + om, map.data(), sizeof(int) * map.size());
     p->owns = false;
     p->d_desc = (GroupDesc *)(w + od);
     p->d_map = (int *)(w + om);
     p->d_counter = (unsigned long long *)(w + oc);
+    const cudaError_t e = cudaMemcpyAsync(w, h, oc, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) {
+      free_plan(p);
+      return cuda_fail(e, "grouped descriptors");
+    }
   }
-  if ((!descs.empty() && cudaMemcpy(p->d_desc, descs.data(), sizeof(GroupDesc) * descs.size(),
-                                    cudaMemcpyHostToDevice) != cudaSuccess) ||
-      (!map.empty() && cudaMemcpy(p->d_map, map.data(), sizeof(int) * map.size(),
-                                  cudaMemcpyHostToDevice) != cudaSuccess)) {
+  if (capture &&
+      ((!descs.empty() && cudaMemcpy(p->d_desc, descs.data(), sizeof(GroupDesc) * descs.size(),
+                                     cudaMemcpyHostToDevice) != cudaSuccess) ||
+       (!map.empty() && cudaMemcpy(p->d_map, map.data(), sizeof(int) * map.size(),
+                                   cudaMemcpyHostToDevice) != cudaSuccess))) {
     free_plan(p);
     return cuda_fail(cudaGetLastError(), "grouped descriptors");
   }
@@ -720,18 +759,22 @@ int make_plan(int count, const b2_gemm_problem *problems, bool capture, Plan **o
 
 int grouped_device(int count, const b2_gemm_problem *problems, cudaStream_t s, int *info) {
   Plan *p = nullptr;
-  int rc = make_plan(count, problems, false, &p, info);
+  int slot = 0;
+  int rc = make_plan(count, problems, false, s, &p, &slot, info);
   if (rc != B2_OK) return rc;
   rc = enqueue(*p, s);
-  // the workspace holding the descriptors is reused by the next call
-  cudaStreamSynchronize(s);
+  // The next call but one that takes this slot waits for this event before
+  // it overwrites the descriptors (and their pinned staging).
+  const cudaError_t e = cudaEventRecord(ctx()->grp_ev[slot], s);
   free_plan(p);
+  if (rc == B2_OK && e != cudaSuccess) rc = cuda_fail(e, "grouped descriptor event");
   return rc;
 }
 
 int grouped_plan_create(int count, const b2_gemm_problem *problems, void **plan, int *info) {
   Plan *p = nullptr;
-  const int rc = make_plan(count, problems, true, &p, info);
+  int slot = 0;
+  const int rc = make_plan(count, problems, true, nullptr, &p, &slot, info);
   if (rc == B2_OK) *plan = p;
   return rc;
 }

@@ -297,7 +297,10 @@ typedef struct b2_gemm_problem {
   double alpha_i, beta_i; /* imaginary parts of alpha and beta (dtypes 2, 3) */
 } b2_gemm_problem;
 
-/* One-shot: upload descriptors, launch, wait for the descriptors to be consumed.
+/* One-shot: build and upload the descriptors (through pinned staging, on
+ * `stream`) and launch; returns once the launch is enqueued, so the caller's
+ * `problems` array may be reused at once.  Consecutive calls alternate two
+ * descriptor slots: a call waits only for the launch two calls back.
  * On an invalid problem returns B2_ERR_ARG with b2_last_info() = its 1-based index. */
 B2_API int b2_gemm_grouped(int count, const b2_gemm_problem *problems, void *stream);
 /* Plan: descriptors uploaded once and "reset queue + launch" captured in a CUDA

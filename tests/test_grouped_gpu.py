@@ -250,3 +250,19 @@ def test_grouped_complex_3m_problems_in_the_same_launch(cuda):
             continue
         err = np.linalg.norm((g - r).astype(np.complex128)) / den
         assert err <= 8, (a.dtype, m, n, k, ta, tb, err)
+
+
+def test_grouped_back_to_back_calls_reuse_descriptor_slots(cuda):
+    """One-shot calls return once enqueued and alternate two descriptor
+    slots: five batches issued back to back on one stream, with no
+    synchronisation in between, all come out right."""
+    import torch
+
+    batches = [make_batch(cuda, 60, 16, 200, seed=40 + i) for i in range(5)]
+    st = torch.cuda.Stream(cuda)
+    L = _lib.lib()
+    for arr, _keep in batches:
+        assert L.b2_gemm_grouped(len(arr), arr, st.cuda_stream) == 0
+    st.synchronize()
+    for _arr, keep in batches:
+        check(keep)
