@@ -10,7 +10,7 @@
 // the owning problem through a tile -> problem map and runs the tile with the
 // problem's own dtype, transposes, strides and alpha/beta:
 //   FP64 tiles: DMMA mma.sync.m16n8k8.f64, 8 warps of 32 x 16;
-//   FP32 tiles: FFMA, 8 warps of 32 x 16, each lane 4 x 4;
+//   FP32 tiles: paired FMAs (fma.rn.f32x2), 8 warps of 32 x 16, each lane 4 x 4;
 //   complex tiles (zgemm3m_ / cgemm3m_ problems): 32 x 32, the three real
 //   products of the 3M method on DMMA (complex128) or FFMA (complex64);
 // warps whose block of a tile lies outside the problem skip their multiplies.
@@ -210,30 +210,42 @@ __device__ void tile_f64(const GroupDesc &g, int m0, int n0, double *sm) {
       }
 }
 
+// Two FP32 FMAs per issued instruction (sm_100 fma.rn.f32x2, each lane
+// rounded as fmaf): c.xy += a.xy * b.xy on 64-bit register pairs.
+__device__ __forceinline__ unsigned long long dup2(float a) {
+  unsigned long long d;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(d) : "f"(a));
+  return d;
+}
+__device__ __forceinline__ void ffma2(unsigned long long &c, unsigned long long a,
+                                      unsigned long long b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(c) : "l"(a), "l"(b));
+}
+
 // FP32 tile: 8 warps of 32 x 16 outputs (the FP64 warp grid), each lane 4 x 4
 // of them: rows 32 (warp / 4) + 4 (lane % 8) + i, columns 16 (warp % 4) +
-// 4 (lane / 8) + j.  A warp whose block lies wholly outside the problem skips
-// its multiplies.
+// 4 (lane / 8) + j, accumulated as column pairs with paired FMAs.  A warp
+// whose block lies wholly outside the problem skips its multiplies.
 __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int rm = (warp >> 2) * 32 + (lane & 7) * 4, cn = (warp & 3) * 16 + (lane >> 3) * 4;
   const bool live = m0 + (warp >> 2) * 32 < g.m && n0 + (warp & 3) * 16 < g.n;
-  float acc[4][4];
+  unsigned long long acc[4][2];  // row i, columns (2 jp, 2 jp + 1)
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+  for (int i = 0; i < 4; ++i) acc[i][0] = acc[i][1] = 0ull;
   tile_k_loop<float>(g, m0, n0, sm, [&](const float *As, const float *Bs) {
     if (!live) return;
 #pragma unroll
     for (int kk = 0; kk < GT_K; ++kk) {
       const float4 a = *reinterpret_cast<const float4 *>(&As[kk * GT_LD + rm]);
-      const float4 b = *reinterpret_cast<const float4 *>(&Bs[kk * GT_LD + cn]);
-      const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+      const ulonglong2 b = *reinterpret_cast<const ulonglong2 *>(&Bs[kk * GT_LD + cn]);
+      const float av[4] = {a.x, a.y, a.z, a.w};
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+      for (int i = 0; i < 4; ++i) {
+        const unsigned long long ai = dup2(av[i]);
+        ffma2(acc[i][0], ai, b.x);
+        ffma2(acc[i][1], ai, b.y);
+      }
     }
   });
   float *C = (float *)g.C;
@@ -242,11 +254,16 @@ __device__ void tile_f32(const GroupDesc &g, int m0, int n0, float *sm) {
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int m = m0 + rm + i, n = n0 + cn + j;
-      if (m < g.m && n < g.n) {
-        float *p = C + (long long)n * g.ldc + m;
-        *p = one ? fmaf(al, acc[i][j], *p) : fmaf(al, acc[i][j], be * *p);
+    for (int jp = 0; jp < 2; ++jp) {
+      const float2 v = *reinterpret_cast<const float2 *>(&acc[i][jp]);
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int m = m0 + rm + i, n = n0 + cn + 2 * jp + e;
+        if (m < g.m && n < g.n) {
+          float *p = C + (long long)n * g.ldc + m;
+          const float x = e ? v.y : v.x;
+          *p = one ? fmaf(al, x, *p) : fmaf(al, x, be * *p);
+        }
       }
     }
 }
