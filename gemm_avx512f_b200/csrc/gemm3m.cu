@@ -1,6 +1,6 @@
 // gemm3m.cu -- complex GEMM by the 3M method.
 //
-// zgemm3m runs in ONE fused launch (zgemm3m_dmma_kernel, FP64 DMMA) below 2^33
+// zgemm3m runs in ONE fused launch (zgemm3m_dmma_kernel, FP64 DMMA) below 2^35
 // multiply-adds and as three FP64 DMMA GEMMs between a pre-add pass and a
 // combine pass above; cgemm3m runs in one fused FFMA launch below 2^24
 // multiply-adds and otherwise as three 3xTF32 tensor-core GEMMs
@@ -612,14 +612,19 @@ int gemm3m_device(char ta, char tb, int m, int n, int k, const T *alpha, const T
   }
   if constexpr (sizeof(T) == 8) {
     // complex128: the one-launch DMMA kernel (16-byte aligned operands, the
-    // normal case; an odd-aligned pointer takes the other paths) below 2^33
-    // multiply-adds.  At 2048^3 the three DMMA GEMMs between a pre-add and a
-    // combine pass run at 38.0 TFLOPS effective against 36.4 for the one
-    // launch (tensor pipe 84 % against 75 % active: the 512-thread fused CTA
-    // holds one CTA per SM); B2_Z3M_FUSED_MAX (multiply-adds) moves the limit.
+    // normal case; an odd-aligned pointer takes the other paths) below 2^35
+    // multiply-adds, 2048^3 included: the pre-adds, the three products and
+    // the combination never leave the SM, and no intermediate planes are
+    // allocated (the three-GEMM form needs 3 (m k + k n + m n) doubles of
+    // workspace, 302 MB at 2048^3).  It runs 4 % below the three DMMA GEMMs
+    // there (36.4 against 38.0 TFLOPS effective; tensor pipe 75 % against 84 %
+    // active: the 512-thread fused CTA holds one CTA per SM).  The three
+    // GEMMs take over from 2^35: at 4096^3 they run at 41.8 TFLOPS effective
+    // against 36.9 for the one launch.  B2_Z3M_FUSED_MAX (multiply-adds)
+    // moves the limit.
     static const double fused_max = [] {
       const char *e = getenv("B2_Z3M_FUSED_MAX");
-      return e ? atof(e) : 8589934592.0;
+      return e ? atof(e) : 34359738368.0;
     }();
     const bool al16 = (((uintptr_t)A | (uintptr_t)B | (uintptr_t)C) & 15) == 0;
     if (al16 && (double)m * n * k < fused_max) {

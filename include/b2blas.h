@@ -120,8 +120,9 @@ B2_API void dtrsm_(const char *side, const char *uplo, const char *transa, const
  * ld in complex elements; trans 'N','T','C' conjugate-transpose,'R' conjugate).
  * Replaces the OpenBLAS gemm3m driver + kernels
  * zgemm3m_kernel_2x8_skylakex.c:336-351 (and the 8x4 variant :309-334) and
- * cgemm3m_kernel_16x4_skylakex.c:415-440.  Products below 2^24 multiply-adds
- * run all three real products and the pre/post additions in one fused launch;
+ * cgemm3m_kernel_16x4_skylakex.c:415-440.  zgemm3m products below 2^35
+ * multiply-adds (2048^3 included) and cgemm3m products below 2^24 run all
+ * three real products and the pre/post additions in one fused launch;
  * larger ones run the three real products as FP64 DMMA GEMMs (zgemm3m) or
  * 3xTF32 tensor-core GEMMs (cgemm3m, FP32-class accuracy) between a pre-add
  * pass and a combine pass. */

@@ -15,7 +15,7 @@ import os
 import numpy as np
 import pytest
 
-from gemm_avx512f_b200 import blas
+from gemm_avx512f_b200 import _lib, blas
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -97,12 +97,12 @@ def test_gemm3m_beta_semantics_and_device_api(cuda):
 
 @pytest.mark.parametrize("ta,tb", [("N", "N"), ("C", "T")])
 def test_zgemm3m_three_gemm_path_large(cuda, ta, tb):
-    """From 2^33 multiply-adds zgemm3m runs three FP64 DMMA GEMMs between a
-    pre-add and a combine pass: 2048^3 against the complex128 product of
+    """From 2^35 multiply-adds zgemm3m runs three FP64 DMMA GEMMs between a
+    pre-add and a combine pass: 4096^3 against the complex128 product of
     torch on the same device (plain FP64 reference of the same op)."""
     import torch
 
-    n = 2048
+    n = 4096
     g = torch.Generator(device=cuda).manual_seed(11)
     A = torch.complex(torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1,
                       torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
@@ -123,6 +123,29 @@ def test_zgemm3m_three_gemm_path_large(cuda, ta, tb):
     den = n * u * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B)) * abs(al)
     err = float(torch.linalg.norm(got - ref)) / den
     assert err <= 8, (ta, tb, err)
+
+
+def test_zgemm3m_config4_size_in_one_launch(cuda):
+    """The configured zgemm3m size, 2048^3 complex128, runs its three real
+    products and the pre/post additions in one launch (the library counts
+    every kernel it launches), against the complex128 product of torch."""
+    import torch
+
+    n = 2048
+    g = torch.Generator(device=cuda).manual_seed(12)
+    A = torch.complex(torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1,
+                      torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
+    B = torch.complex(torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1,
+                      torch.rand(n, n, device=cuda, dtype=torch.float64, generator=g) * 2 - 1)
+    C = torch.zeros(n, n, device=cuda, dtype=torch.complex128)
+    torch.cuda.synchronize()
+    n0 = _lib.launch_count()
+    blas.zgemm3m_device("N", "N", n, n, n, 1.0, A, n, B, n, 0.0, C, n)
+    torch.cuda.synchronize()
+    assert _lib.launch_count() - n0 == 1
+    ref = A.t() @ B.t()
+    den = n * 2.0 ** -53 * float(torch.linalg.norm(A)) * float(torch.linalg.norm(B))
+    assert float(torch.linalg.norm(C.t() - ref)) / den <= 8
 
 
 _FUSED_SCRIPT = """
