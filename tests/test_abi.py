@@ -144,3 +144,26 @@ def test_dgemm_multi_argument_errors(ndev, devs, args, info):
     assert st == _lib.B2_ERR_ARG
     assert _lib.lib().b2_last_info() == info
     assert (c == 3.0).all()
+
+
+def test_problem_struct_layout_matches_the_header(tmp_path):
+    """b2_gemm_problem as a C compiler lays it out from include/b2blas.h (gcc
+    here) and the ctypes mirror the Python bindings pass to
+    b2_gemm_grouped: same size and the same offset for every field."""
+    import os
+
+    hdr = os.path.dirname(_lib.HEADER)
+    fields = [f[0] for f in _lib.GemmProblem._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"b2blas.h\"\n"
+                   "int main(void) {\n  printf(\"size %zu\\n\", sizeof(b2_gemm_problem));\n"
+                   + "".join(f"  printf(\"{f} %zu\\n\", offsetof(b2_gemm_problem, {f}));\n"
+                             for f in fields)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", hdr, str(src), "-o", str(exe)], check=True)
+    out = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                  check=True).stdout.splitlines())
+    assert int(out["size"]) == C.sizeof(_lib.GemmProblem)
+    for f in fields:
+        assert int(out[f]) == getattr(_lib.GemmProblem, f).offset, f
