@@ -167,3 +167,39 @@ def test_problem_struct_layout_matches_the_header(tmp_path):
     assert int(out["size"]) == C.sizeof(_lib.GemmProblem)
     for f in fields:
         assert int(out[f]) == getattr(_lib.GemmProblem, f).offset, f
+
+
+def test_unchanged_c_caller_links_against_the_library(tmp_path):
+    """A C program written against the reference's dgemm_ (the prototype of
+    src/gemm_driver.c:116) links against libb2blas.so as the integration
+    notes show, and sees BLAS argument checking through b2_last_error /
+    b2_last_info (no device is needed before the arguments are valid)."""
+    import os
+
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    src = tmp_path / "app.c"
+    src.write_text(r"""
+#include <stdio.h>
+extern void dgemm_(const char*, const char*, const int*, const int*, const int*,
+                   const double*, const double*, const int*, const double*, const int*,
+                   const double*, double*, const int*);
+extern int b2_last_error(void);
+extern int b2_last_info(void);
+int main(void) {
+  double a[4] = {1, 2, 3, 4}, b[4] = {1, 0, 0, 1}, c[4] = {7, 7, 7, 7};
+  double alpha = 1.0, beta = 0.0;
+  int m = -1, n = 2, k = 2, lda = 2, ldb = 2, ldc = 2;
+  dgemm_("N", "N", &m, &n, &k, &alpha, a, &lda, b, &ldb, &beta, c, &ldc);
+  printf("bad_m %d %d %g\n", b2_last_error(), b2_last_info(), c[0]);
+  m = 2; lda = 1;
+  dgemm_("N", "N", &m, &n, &k, &alpha, a, &lda, b, &ldb, &beta, c, &ldc);
+  printf("bad_lda %d %d %g\n", b2_last_error(), b2_last_info(), c[0]);
+  return 0;
+}
+""")
+    exe = tmp_path / "app"
+    subprocess.run(["gcc", str(src), "-o", str(exe), f"-L{libdir}", "-lb2blas",
+                    f"-Wl,-rpath,{libdir}"], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    assert out[0].split() == ["bad_m", str(_lib.B2_ERR_ARG), "3", "7"]
+    assert out[1].split() == ["bad_lda", str(_lib.B2_ERR_ARG), "8", "7"]
