@@ -78,6 +78,10 @@ int sgemm_simt(char ta, char tb, int m, int n, int k, float alpha, const float *
 // (row pitch 2 kp floats), the layout the tensor-core engine reads.
 int sgemm_split_tf32x3(const float *X, long long sr, long long sk, int R, int K, int kp,
                        float *out, cudaStream_t s);
+// C(m, n) = alpha * sum_ks W[ks * plane + n * ldw + m] + beta C (beta != 1
+// multiplies), the S partials summed in FP64 in K order and rounded once.
+int sgemm_splitk_reduce(const float *W, long long plane, int ldw, int S, int m, int n,
+                        float alpha, float beta, float *C, int ldc, cudaStream_t s);
 
 // Blocked triangular solve (trsm.cu).
 int dtrsm_device(char side, char uplo, char transa, char diag, int m, int n, double alpha,

@@ -57,16 +57,20 @@ __device__ __forceinline__ float4 load4(const float *p, int lim) {
   return v;
 }
 
-template <bool TA, bool TB, bool VEC>
+template <bool TA, bool TB, bool VEC, bool SPLIT>
 __global__ void __launch_bounds__(256, 2)
     sgemm_ffma2_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, int lda,
                        const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
-                       int ldc) {
+                       int ldc, int kchunk, float *__restrict__ P, long long plane, int ldp) {
   extern __shared__ __align__(16) float s2mem[];
   float *As = s2mem;                        // [2][S2_K][S2_ALD]
   float *Bs = s2mem + 2 * S2_K * S2_ALD;    // [2][S2_K][S2_BLD]
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int m0 = blockIdx.x * S2_M, n0 = blockIdx.y * S2_N;
+  // K range of this CTA: all of K, or (SPLIT) slice blockIdx.z of a split-K
+  // launch (kchunk a multiple of S2_K), whose raw sums go to P + z * plane.
+  const int kbeg = SPLIT ? blockIdx.z * kchunk : 0;
+  const int kend = SPLIT ? min(K, kbeg + kchunk) : K;
 
   unsigned long long acc[8][4];  // row r: 4tx + (r&3) + 64(r>>2); column pair c
 #pragma unroll
@@ -84,17 +88,17 @@ __global__ void __launch_bounds__(256, 2)
       const int c = tid + 256 * h;
       if (!TA) {  // 4 consecutive m of one k
         const int kk = c >> 5, mm = (c & 31) * 4, gm = m0 + mm, gk = k0 + kk;
-        ra[h] = gk < K ? load4<VEC>(A + (size_t)gk * lda + gm, M - gm) : make_float4(0.f, 0.f, 0.f, 0.f);
+        ra[h] = gk < kend ? load4<VEC>(A + (size_t)gk * lda + gm, M - gm) : make_float4(0.f, 0.f, 0.f, 0.f);
       } else {    // 4 consecutive k of one m
         const int mm = c >> 2, kk = (c & 3) * 4, gm = m0 + mm, gk = k0 + kk;
-        ra[h] = gm < M ? load4<VEC>(A + (size_t)gm * lda + gk, K - gk) : make_float4(0.f, 0.f, 0.f, 0.f);
+        ra[h] = gm < M ? load4<VEC>(A + (size_t)gm * lda + gk, kend - gk) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
       if (TB) {   // 4 consecutive n of one k
         const int kk = c >> 5, nn = (c & 31) * 4, gn = n0 + nn, gk = k0 + kk;
-        rb[h] = gk < K ? load4<VEC>(B + (size_t)gk * ldb + gn, N - gn) : make_float4(0.f, 0.f, 0.f, 0.f);
+        rb[h] = gk < kend ? load4<VEC>(B + (size_t)gk * ldb + gn, N - gn) : make_float4(0.f, 0.f, 0.f, 0.f);
       } else {    // 4 consecutive k of one n
         const int nn = c >> 2, kk = (c & 3) * 4, gn = n0 + nn, gk = k0 + kk;
-        rb[h] = gn < N ? load4<VEC>(B + (size_t)gn * ldb + gk, K - gk) : make_float4(0.f, 0.f, 0.f, 0.f);
+        rb[h] = gn < N ? load4<VEC>(B + (size_t)gn * ldb + gk, kend - gk) : make_float4(0.f, 0.f, 0.f, 0.f);
       }
     }
   };
@@ -125,13 +129,13 @@ __global__ void __launch_bounds__(256, 2)
     }
   };
 
-  const int KT = (K + S2_K - 1) / S2_K;
-  gload(0);
+  const int KT = (kend - kbeg + S2_K - 1) / S2_K;
+  gload(kbeg);
   sstore(0);
   __syncthreads();
   for (int kt = 0; kt < KT; ++kt) {
     const int buf = kt & 1;
-    if (kt + 1 < KT) gload((kt + 1) * S2_K);
+    if (kt + 1 < KT) gload(kbeg + (kt + 1) * S2_K);
     const float *as = As + buf * S2_K * S2_ALD;
     const float *bs = Bs + buf * S2_K * S2_BLD;
 #pragma unroll
@@ -179,24 +183,72 @@ __global__ void __launch_bounds__(256, 2)
       for (int e = 0; e < 2; ++e) {
         const int n = nb + e;
         if (n >= N) continue;
-        float *p = C + (size_t)n * ldc + m;
         const float x = e ? v.y : v.x;
+        if (SPLIT) {
+          P[blockIdx.z * plane + (long long)n * ldp + m] = x;
+          continue;
+        }
+        float *p = C + (size_t)n * ldc + m;
         *p = beta_one ? fmaf(alpha, x, *p) : fmaf(alpha, x, beta * *p);
       }
     }
   }
 }
 
+// K slices for a grid of `tiles` CTAs at two per SM: 1 when the tiles fill
+// the slots, else the count (at most 8, each slice >= 32 K blocks of 16)
+// whose work units best fill whole waves of 2 * sms.  8192 x 256 x 8192 has
+// 128 tiles for the 296 slots of 148 SMs; 2 slices fill them 86 %.
+int ffma2_ksplit(long long tiles, int kblocks, int sms) {
+  const long long slots = 2ll * sms;
+  if (tiles >= slots) return 1;
+  int best = 1;
+  double best_eff = (double)tiles / slots;
+  for (int S = 2; S <= 8 && S * 32 <= kblocks; ++S) {
+    const long long units = tiles * S, waves = (units + slots - 1) / slots;
+    const double eff = (double)units / (double)(waves * slots);
+    if (eff > best_eff + 0.02) {
+      best = S;
+      best_eff = eff;
+    }
+  }
+  return best;
+}
+
 template <bool TA, bool TB, bool VEC>
 int launch_ffma2(int m, int n, int k, float alpha, const float *A, int lda, const float *B,
                  int ldb, float beta, float *C, int ldc, cudaStream_t s) {
-  auto kern = sgemm_ffma2_kernel<TA, TB, VEC>;
-  B2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM));
-  dim3 grid((m + S2_M - 1) / S2_M, (n + S2_N - 1) / S2_N);
-  B2_PROF("sgemm_simt", s);
-  kern<<<grid, 256, S2_SMEM, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
-  B2_CUDA_TRY(cudaGetLastError());
-  return B2_OK;
+  auto kern = sgemm_ffma2_kernel<TA, TB, VEC, false>;
+  auto kern_split = sgemm_ffma2_kernel<TA, TB, VEC, true>;
+  Ctx *cx = ctx();
+  if (!cx) return B2_ERR_NO_DEVICE;
+  const int gx = (m + S2_M - 1) / S2_M, gy = (n + S2_N - 1) / S2_N;
+  const int kblocks = (k + S2_K - 1) / S2_K;
+  const int S = ffma2_ksplit((long long)gx * gy, kblocks, cx->sm_count);
+  if (S == 1) {
+    B2_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM));
+    B2_PROF("sgemm_simt", s);
+    kern<<<dim3(gx, gy), 256, S2_SMEM, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, k,
+                                             nullptr, 0, 0);
+    B2_CUDA_TRY(cudaGetLastError());
+    return B2_OK;
+  }
+  // Split-K: S raw partial products of K ranges (multiples of S2_K), then one
+  // reduction adding them in K order (FP64 sums, rounded once) into C.
+  const int kchunk = (kblocks + S - 1) / S * S2_K;
+  const int S_used = (k + kchunk - 1) / kchunk;
+  const long long plane = (long long)n * m;
+  float *P = (float *)workspace(cx, WS_MISC, (size_t)plane * S_used * sizeof(float));
+  if (!P) return B2_ERR_NOMEM;
+  {
+    B2_CUDA_TRY(
+        cudaFuncSetAttribute(kern_split, cudaFuncAttributeMaxDynamicSharedMemorySize, S2_SMEM));
+    B2_PROF("sgemm_simt", s);
+    kern_split<<<dim3(gx, gy, S_used), 256, S2_SMEM, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C,
+                                                           ldc, kchunk, P, plane, m);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
+  return sgemm_splitk_reduce(P, plane, m, S_used, m, n, alpha, beta, C, ldc, s);
 }
 
 }  // namespace

@@ -370,6 +370,11 @@ int sgemm_tensor_cfg(char ta, char tb, int m, int n, int k, float alpha, const f
   F32PartialEpi pe{W, plane, ldw, m, n};
   rc = run(pe);
   if (rc != B2_OK) return rc;
+  return sgemm_splitk_reduce(W, plane, ldw, S, m, n, alpha, beta, C, ldc, s);
+}
+
+int sgemm_splitk_reduce(const float *W, long long plane, int ldw, int S, int m, int n,
+                        float alpha, float beta, float *C, int ldc, cudaStream_t s) {
   dim3 grid((unsigned)((m + 255) / 256), (unsigned)(n < 4096 ? n : 4096));
   B2_PROF("sgemm_splitk_reduce", s);
   sgemm_splitk_reduce_kernel<<<grid, 256, 0, s>>>(W, plane, ldw, S, m, n, alpha, beta, C, ldc);
