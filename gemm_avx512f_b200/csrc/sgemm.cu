@@ -62,15 +62,25 @@ __global__ void __launch_bounds__(256, 2)
     sgemm_ffma2_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, int lda,
                        const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
                        int ldc, int kchunk, float *__restrict__ P, long long plane, int ldp) {
+  // Slice blockIdx.z of a split-K launch reads its own K range.  Transposed-A
+  // instances shift the operand bases and shorten K (fewer live registers
+  // for them); the others keep K and bound the range by kbeg / kend.
+  constexpr bool SHIFT = SPLIT && TA;
+  if (SHIFT) {
+    const int kb = blockIdx.z * kchunk;
+    A += (size_t)kb;
+    B += TB ? (size_t)kb * ldb : (size_t)kb;
+    K = min(kchunk, K - kb);
+  }
   extern __shared__ __align__(16) float s2mem[];
   float *As = s2mem;                        // [2][S2_K][S2_ALD]
   float *Bs = s2mem + 2 * S2_K * S2_ALD;    // [2][S2_K][S2_BLD]
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int m0 = blockIdx.x * S2_M, n0 = blockIdx.y * S2_N;
-  // K range of this CTA: all of K, or (SPLIT) slice blockIdx.z of a split-K
-  // launch (kchunk a multiple of S2_K), whose raw sums go to P + z * plane.
-  const int kbeg = SPLIT ? blockIdx.z * kchunk : 0;
-  const int kend = SPLIT ? min(K, kbeg + kchunk) : K;
+  // K range of this CTA (kchunk a multiple of S2_K); a split-K slice writes
+  // its raw sums to P + z * plane.
+  const int kbeg = (SPLIT && !SHIFT) ? blockIdx.z * kchunk : 0;
+  const int kend = (SPLIT && !SHIFT) ? min(K, kbeg + kchunk) : K;
 
   unsigned long long acc[8][4];  // row r: 4tx + (r&3) + 64(r>>2); column pair c
 #pragma unroll
