@@ -62,15 +62,23 @@ __global__ void __launch_bounds__(256, 2)
     sgemm_ffma2_kernel(int M, int N, int K, float alpha, const float *__restrict__ A, int lda,
                        const float *__restrict__ B, int ldb, float beta, float *__restrict__ C,
                        int ldc, int kchunk, float *__restrict__ P, long long plane, int ldp) {
-  // Slice blockIdx.z of a split-K launch reads its own K range.  Transposed-A
-  // instances shift the operand bases and shorten K (fewer live registers
-  // for them); the others keep K and bound the range by kbeg / kend.
-  constexpr bool SHIFT = SPLIT && TA;
+  // Slice blockIdx.z of a split-K launch reads its own K range: either the
+  // operand bases shift to it and K shortens (SHIFT), or K stays and kbeg /
+  // kend bound the range.  The form per transpose pair is the one ptxas
+  // compiles with the fewest spilled registers (NN shifts by 64-bit offsets).
+  constexpr bool SHIFT = SPLIT && (TA || !TB);
   if (SHIFT) {
-    const int kb = blockIdx.z * kchunk;
-    A += (size_t)kb;
-    B += TB ? (size_t)kb * ldb : (size_t)kb;
-    K = min(kchunk, K - kb);
+    if (TA) {
+      const int kb = blockIdx.z * kchunk;
+      A += (size_t)kb;
+      B += TB ? (size_t)kb * ldb : (size_t)kb;
+      K = min(kchunk, K - kb);
+    } else {
+      const long long kb = (long long)blockIdx.z * kchunk;
+      A += kb * lda;
+      B += kb;
+      K = min(kchunk, K - (int)kb);
+    }
   }
   extern __shared__ __align__(16) float s2mem[];
   float *As = s2mem;                        // [2][S2_K][S2_ALD]
