@@ -286,3 +286,39 @@ def test_grouped_3m_panels_and_warp_blocks():
         assert rm // 16 == warp >> 2 and cn // 8 == warp & 3
         owned |= {(rm + i, cn + j) for i in range(2) for j in range(2)}
     assert owned == {(m, n) for m in range(32) for n in range(32)}
+
+
+# ------------------------------------------------ FP32 CUDA-core split-K ----
+def ffma2_ksplit(tiles, kblocks, sms=148):
+    slots = 2 * sms
+    if tiles >= slots:
+        return 1
+    best, best_eff = 1, tiles / slots
+    for S in range(2, 9):
+        if S * 32 > kblocks:
+            break
+        units = tiles * S
+        waves = -(-units // slots)
+        eff = units / (waves * slots)
+        if eff > best_eff + 0.02:
+            best, best_eff = S, eff
+    return best
+
+
+def test_ffma2_split_slices_cover_k_once():
+    # slices of kchunk (a multiple of the 16-deep K block) cover [0, K) once,
+    # none empty; grids that fill the 296 slots stay unsplit
+    for m, n, k in [(8192, 256, 8192), (2048, 160, 1536), (1024, 1024, 1024), (4096, 4096, 4096),
+                    (513, 129, 1031), (100, 100, 5000), (16, 16, 16), (128, 128, 513)]:
+        tiles = -(-m // 128) * -(-n // 128)
+        kblocks = -(-k // 16)
+        S = ffma2_ksplit(tiles, kblocks)
+        assert 1 <= S <= 8 and (S == 1 or tiles < 296)
+        kchunk = -(-kblocks // S) * 16
+        used = -(-k // kchunk)
+        ranges = [(z * kchunk, min(k, (z + 1) * kchunk)) for z in range(used)]
+        assert kchunk % 16 == 0 and all(a < b for a, b in ranges)
+        assert ranges[0][0] == 0 and ranges[-1][1] == k
+        assert all(ranges[i][1] == ranges[i + 1][0] for i in range(used - 1))
+        if S > 1:
+            assert min(b - a for a, b in ranges[:-1]) >= 512
